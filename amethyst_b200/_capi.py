@@ -1,0 +1,90 @@
+"""ctypes view of the C ABI declared in include/amethyst.h.
+
+The shared library is built in-tree (amethyst_b200/libamethyst_b200.so, see build.py).  There
+is no fallback: if the library is missing or fails to load, importing the operators raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PLAIN32, PLAIN64, SLAB, NOGAPS = 0, 1, 2, 3
+FORMAT_NAMES = {PLAIN32: "plain32", PLAIN64: "plain64", SLAB: "slab", NOGAPS: "nogaps"}
+
+(PRED_ALL, PRED_LT, PRED_LE, PRED_GT, PRED_GE, PRED_EQ, PRED_NE, PRED_BETWEEN, PRED_NOT_BETWEEN,
+ PRED_HALF) = range(10)
+
+(OP_ADD, OP_SUB, OP_MUL, OP_DIV, OP_MOD, OP_MIN, OP_MAX, OP_AND, OP_OR, OP_XOR, OP_BOOL_OR,
+ OP_BOOL_XOR, OP_MATH, OP_LHS) = range(14)
+
+AGG_SUM, AGG_MIN, AGG_MAX, AGG_AND, AGG_OR, AGG_XOR = range(6)
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "unsupported", 3: "misaligned pointer",
+    4: "workspace too small", 5: "CUDA error", 6: "device-side wait timed out",
+    7: "size exceeds capacity",
+}
+
+
+class Column(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("n", C.c_uint64), ("format", C.c_uint32), ("bits", C.c_uint32)]
+
+
+class Predicate(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("bits", C.c_uint32), ("k0", C.c_uint64), ("k1", C.c_uint64)]
+
+
+class ChainDesc(C.Structure):
+    _fields_ = [("op", C.c_uint32), ("value_bits", C.c_uint32), ("pred", Predicate),
+                ("agg", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libamethyst_b200.so")
+
+_P = C.c_void_p
+_COL = C.POINTER(Column)
+_SIGS = {
+    "amx_version": (C.c_int, []),
+    "amx_status_string": (C.c_char_p, [C.c_int]),
+    "amx_last_error": (C.c_char_p, []),
+    "amx_storage_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint64]),
+    "amx_mask_bytes": (C.c_uint64, [C.c_uint64]),
+    "amx_binary_out_bits": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32]),
+    "amx_workspace_bytes": (C.c_uint64, [C.c_uint64]),
+    "amx_workspace_status": (C.c_int, [_P, _P]),
+    "amx_filter": (C.c_int, [_COL, C.POINTER(Predicate), _P, _P, C.c_size_t, _P]),
+    "amx_compressstore": (C.c_int, [_COL, _P, _COL, _P, _P, C.c_size_t, _P]),
+    "amx_filter_compressstore": (C.c_int, [_COL, C.POINTER(Predicate), _COL, _P, _P, C.c_size_t, _P]),
+    "amx_binary": (C.c_int, [C.c_uint32, _COL, _COL, _COL, _P, C.c_size_t, _P]),
+    "amx_convert": (C.c_int, [_COL, _COL, _P, C.c_size_t, _P]),
+    "amx_reduce": (C.c_int, [C.c_uint32, _COL, _P, _P, _P, C.c_size_t, _P]),
+    "amx_chain": (C.c_int, [C.POINTER(ChainDesc), _COL, _COL, _COL, _P, _P, _P, _P, C.c_size_t, _P]),
+}
+
+_lib = None
+
+
+class AmxError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def lib():
+    """Load libamethyst_b200.so once; raise if it is absent (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run amethyst_b200.build.build() first")
+        h = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = h
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise AmxError(status, lib().amx_last_error().decode())

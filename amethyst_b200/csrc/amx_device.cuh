@@ -1,0 +1,285 @@
+// amx_device.cuh -- device building blocks shared by the Amethyst B200 kernels:
+// mbarrier + bulk-copy (TMA) staging, bounded waits, look-back status words, predicate and
+// operator evaluation, and the per-format element readers.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "amx_internal.h"
+
+namespace amx {
+
+// ---------------------------------------------------------------------------------------------
+// shared-memory addresses, mbarriers and 1-D bulk copies (cp.async.bulk, no multicast)
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// global -> shared bulk copy completing on an mbarrier; dst, src 16-byte aligned, bytes % 16 == 0
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Bounded wait on an mbarrier phase.  Returns false when the limit ran out; the caller
+// records AMX_ERR_TIMEOUT and stops using the stage.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < kWaitSpins; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// look-back status words: [63:62] flag, [61:0] value
+// ---------------------------------------------------------------------------------------------
+constexpr uint64_t kFlagAgg = 1ull << 62;
+constexpr uint64_t kFlagInc = 2ull << 62;
+constexpr uint64_t kValMask = (1ull << 62) - 1;
+
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v)
+{
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p)
+{
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void record_error(uint32_t* err, uint32_t code) { atomicCAS(err, 0u, code); }
+
+// Decoupled look-back (single-pass chained scan).  Called by all 32 lanes of one warp with
+// the tile's survivor count; returns the number of survivors in all earlier tiles.  Every
+// wait is bounded: on timeout the error word is set and the missing prefix is taken as 0.
+__device__ __forceinline__ uint64_t lookback(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t* err)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st_relaxed_u64(&status[0], kFlagInc | agg);
+        return 0;
+    }
+    if (lane == 0) st_relaxed_u64(&status[tile], kFlagAgg | agg);
+    uint64_t excl = 0;
+    int64_t j = (int64_t)tile - 1;
+    while (true) {
+        const int64_t idx = j - (int64_t)lane;
+        uint64_t st = kFlagInc;  // before tile 0: an inclusive prefix of 0
+        if (idx >= 0) {
+            uint32_t spins = 0;
+            st = ld_relaxed_u64(&status[idx]);
+            while ((st >> 62) == 0) {
+                if (++spins > kWaitSpins) {
+                    record_error(err, AMX_ERR_TIMEOUT);
+                    st = kFlagInc;
+                    break;
+                }
+                if (spins > 32) __nanosleep(32);
+                st = ld_relaxed_u64(&status[idx]);
+            }
+        }
+        const uint32_t inc = __ballot_sync(0xffffffffu, (st >> 62) == 2);
+        const int first = __ffs(inc) - 1;
+        uint64_t v = st & kValMask;
+        if (first >= 0 && (int)lane > first) v = 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (first >= 0) break;
+        j -= 32;
+    }
+    if (lane == 0) st_relaxed_u64(&status[tile], kFlagInc | (excl + agg));
+    return excl;
+}
+
+// ---------------------------------------------------------------------------------------------
+// predicate and operator evaluation
+// ---------------------------------------------------------------------------------------------
+// A predicate normalised on the host to  keep(v) = ((v - lo) <= span) != neg.
+struct PredN {
+    uint64_t lo;
+    uint64_t span;
+    uint32_t neg;
+    uint32_t pad;
+};
+
+template <typename V>
+__device__ __forceinline__ bool pred_eval(const PredN& p, V v)
+{
+    return (((uint64_t)v - p.lo) <= p.span) != (p.neg != 0);
+}
+
+__device__ __forceinline__ uint64_t binop_eval(uint32_t op, uint64_t l, uint64_t r)
+{
+    switch (op) {
+        case AMX_OP_ADD: return l + r;
+        case AMX_OP_SUB: return l - r;
+        case AMX_OP_MUL: return l * r;
+        case AMX_OP_DIV: return r ? l / r : ~0ull;
+        case AMX_OP_MOD: return r ? l % r : l;
+        case AMX_OP_MIN: return l < r ? l : r;
+        case AMX_OP_MAX: return l > r ? l : r;
+        case AMX_OP_AND: return l & r;
+        case AMX_OP_OR: return l | r;
+        case AMX_OP_XOR: return l ^ r;
+        case AMX_OP_BOOL_OR: return (l || r) ? 1ull : 0ull;
+        case AMX_OP_BOOL_XOR: return ((l && !r) || (!l && r)) ? 1ull : 0ull;
+        case AMX_OP_MATH: {
+            const uint64_t den = l * l + r * r + 5 * l;
+            return den ? (l * l + r * r + 4 * l) / den : ~0ull;
+        }
+        default: return l;
+    }
+}
+
+// Aggregations are kept in an encoded form so that every one of them has identity 0 and a
+// native 64-bit atomic: min(x) = ~max(~x), and(x) = ~or(~x).
+__device__ __forceinline__ uint64_t agg_encode(uint32_t agg, uint64_t v)
+{
+    return (agg == AMX_AGG_MIN || agg == AMX_AGG_AND) ? ~v : v;
+}
+__device__ __forceinline__ uint64_t agg_combine(uint32_t agg, uint64_t a, uint64_t e)
+{
+    switch (agg) {
+        case AMX_AGG_SUM: return a + e;
+        case AMX_AGG_MIN:
+        case AMX_AGG_MAX: return a > e ? a : e;
+        case AMX_AGG_AND:
+        case AMX_AGG_OR: return a | e;
+        case AMX_AGG_XOR: return a ^ e;
+    }
+    return a;
+}
+__device__ __forceinline__ void agg_atomic(uint32_t agg, unsigned long long* p, uint64_t e)
+{
+    switch (agg) {
+        case AMX_AGG_SUM: atomicAdd(p, (unsigned long long)e); break;
+        case AMX_AGG_MIN:
+        case AMX_AGG_MAX: atomicMax(p, (unsigned long long)e); break;
+        case AMX_AGG_AND:
+        case AMX_AGG_OR: atomicOr(p, (unsigned long long)e); break;
+        case AMX_AGG_XOR: atomicXor(p, (unsigned long long)e); break;
+    }
+}
+__device__ __forceinline__ uint64_t agg_decode(uint32_t agg, uint64_t a)
+{
+    return (agg == AMX_AGG_MIN || agg == AMX_AGG_AND) ? ~a : a;
+}
+
+__device__ __forceinline__ uint64_t mask_bits(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1); }
+
+// ---------------------------------------------------------------------------------------------
+// runtime-width streaming reader over a staged copy of one column (shared memory)
+// ---------------------------------------------------------------------------------------------
+// `base` is the staged bytes; `first` is the column element the stream starts at and `sbyte`
+// the column byte offset the stage starts at.
+struct Stream {
+    const uint8_t* base;
+    uint64_t cur;   // slab: remaining fields; nogaps: low word of the window
+    uint64_t nxt;   // nogaps: high word of the window
+    uint32_t word;  // index of the current 8-byte word (slab/nogaps) or element (plain)
+    uint32_t left;  // slab: fields left in cur; nogaps: bit offset in the window
+    uint32_t fmt, bits, eps;
+    uint64_t m;
+
+    __device__ __forceinline__ void init(const ColDev& c, const uint8_t* stage, uint64_t sbyte, uint64_t first)
+    {
+        base = stage;
+        fmt = c.format;
+        bits = c.bits;
+        eps = c.eps;
+        m = c.mask;
+        const uint64_t* w = reinterpret_cast<const uint64_t*>(stage);
+        switch (fmt) {
+            case AMX_PLAIN32: word = (uint32_t)(first - sbyte / 4); break;
+            case AMX_PLAIN64: word = (uint32_t)(first - sbyte / 8); break;
+            case AMX_SLAB: {
+                const uint64_t s = first / eps;
+                const uint32_t k = (uint32_t)(first - s * eps);
+                word = (uint32_t)(s - sbyte / 8);
+                cur = k ? (w[word] >> (k * bits)) : w[word];
+                left = eps - k;
+                break;
+            }
+            default: {  // nogaps
+                const uint64_t bitpos = first * bits - sbyte * 8;
+                word = (uint32_t)(bitpos >> 6);
+                left = (uint32_t)(bitpos & 63);
+                cur = w[word];
+                nxt = w[word + 1];
+                break;
+            }
+        }
+    }
+
+    __device__ __forceinline__ uint64_t next()
+    {
+        const uint64_t* w = reinterpret_cast<const uint64_t*>(base);
+        uint64_t v;
+        switch (fmt) {
+            case AMX_PLAIN32: v = reinterpret_cast<const uint32_t*>(base)[word++]; break;
+            case AMX_PLAIN64: v = w[word++]; break;
+            case AMX_SLAB:
+                v = cur;
+                cur = bits < 64 ? (cur >> bits) : 0;
+                if (--left == 0) {
+                    cur = w[++word];
+                    left = eps;
+                }
+                break;
+            default: {
+                const uint32_t off = left;
+                v = off ? ((cur >> off) | (nxt << (64 - off))) : cur;
+                const uint32_t e = off + bits;
+                if (e >= 64) {
+                    cur = nxt;
+                    nxt = w[++word + 1];
+                    left = e - 64;
+                }
+                else {
+                    left = e;
+                }
+                break;
+            }
+        }
+        return v & m;
+    }
+};
+
+}  // namespace amx

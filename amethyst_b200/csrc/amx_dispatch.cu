@@ -1,0 +1,118 @@
+// amx_dispatch.cu -- builds the tile-pipeline parameters for a request, picks the decode
+// policy, clears the workspace and launches the persistent grid.
+#include "amx_dispatch.h"
+#include "amx_pipeline.cuh"
+#include "amx_policies.cuh"
+
+namespace amx {
+
+static uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+// shared-memory bytes to stage one tile of column c (tile_elems elements), with 16 bytes of
+// alignment shift and 32 bytes of read-ahead slack
+static uint32_t stage_need(const ColDev& c, uint32_t tile_elems)
+{
+    uint64_t b = 0;
+    switch (c.format) {
+        case AMX_PLAIN32: b = 4ull * tile_elems; break;
+        case AMX_PLAIN64: b = 8ull * tile_elems; break;
+        case AMX_SLAB: b = 8ull * (tile_elems / c.eps + 2); break;
+        case AMX_NOGAPS: b = 8ull * ((uint64_t)tile_elems * c.bits / 64 + 2); break;
+        default: b = tile_elems / 8 + 8; break;
+    }
+    return round_up((uint32_t)b + 48, 128);
+}
+
+template <class Pol>
+static amx_status launch(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
+{
+    constexpr uint32_t TILE = kPipeThreads * Pol::R;
+    p.tile_elems = TILE;
+    p.num_tiles = (p.n + TILE - 1) / TILE;
+    const uint64_t need = sizeof(WsHeader) + 8 * p.num_tiles;
+    if (!ws) return fail(AMX_ERR_WORKSPACE, "workspace is null");
+    if (ws_bytes < need)
+        return fail(AMX_ERR_WORKSPACE, "workspace of %zu bytes, %llu needed", ws_bytes, (unsigned long long)need);
+    if (((uintptr_t)ws) & 15) return fail(AMX_ERR_ALIGNMENT, "workspace not 16-byte aligned");
+    p.ws = reinterpret_cast<WsHeader*>(ws);
+    p.status = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(ws) + sizeof(WsHeader));
+
+    p.a_off = 0;
+    uint32_t off = stage_need(p.a, TILE);
+    p.b_off = off;
+    if (p.has_b) off += stage_need(p.b, TILE);
+    p.m_off = off;
+    if (p.has_mask_in) off += stage_need(p.m, TILE);
+    p.stage_bytes = off;
+    p.smem_fixed = p.has_out ? round_up(kCvOff + TILE * (uint32_t)sizeof(typename Pol::V), 128) : kCvOff;
+    const uint32_t smem = p.smem_fixed + kStages * p.stage_bytes;
+    if (smem > 227 * 1024) return fail(AMX_ERR_UNSUPPORTED, "pipeline needs %u bytes of shared memory", smem);
+
+    cudaError_t e = cudaMemsetAsync(ws, 0, need, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "workspace clear");
+    auto kern = pipe_kernel<Pol>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "shared memory attribute");
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPipeThreads, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "occupancy");
+    if (per_sm < 1) return fail(AMX_ERR_UNSUPPORTED, "pipeline kernel does not fit on an SM");
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > p.num_tiles) grid = p.num_tiles;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, kPipeThreads, smem, stream>>>(p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "pipeline launch");
+    return AMX_OK;
+}
+
+amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t stream)
+{
+    PipeParams p{};
+    p.a = col_dev(r.a);
+    p.n = r.a->n;
+    if (r.b) {
+        p.b = col_dev(r.b);
+        p.has_b = 1;
+    }
+    if (r.mask_in) {
+        p.m = mask_dev(r.mask_in, p.n);
+        p.has_mask_in = 1;
+    }
+    if (r.out) {
+        p.out = out_dev(r.out);
+        p.has_out = 1;
+        p.compact = r.compact;
+    }
+    p.op = r.b ? r.op : AMX_OP_LHS;
+    p.vbits = r.vbits;
+    p.vmask = mask_of(r.vbits);
+    if (r.pred) {
+        amx_status st = normalize_pred(r.pred, p.pred_lo, p.pred_span, p.pred_neg);
+        if (st) return st;
+        p.has_pred = 1;
+        // for values below 2^32 the range test is exact in 32-bit arithmetic when the range
+        // starts below 2^32 and does not wrap
+        if (p.pred_lo < (1ull << 32) && p.pred_lo + p.pred_span >= p.pred_lo) {
+            const uint64_t room = 0xffffffffull - p.pred_lo;
+            p.pred_lo32 = (uint32_t)p.pred_lo;
+            p.pred_span32 = (uint32_t)(p.pred_span < room ? p.pred_span : room);
+            p.pred32_ok = 1;
+        }
+    }
+    p.agg = r.agg;
+    p.has_agg = r.has_agg;
+    p.mask_out = r.mask_out;
+    p.count_out = r.count_out;
+    p.agg_out = r.agg_out;
+
+    switch (choose_policy(p, r.force_policy)) {
+#define AMX_POLICY_CASE(id, Pol) \
+    case id: return launch<Pol>(p, ws, ws_bytes, stream);
+        AMX_POLICY_LIST(AMX_POLICY_CASE)
+#undef AMX_POLICY_CASE
+        default: return launch<GenericPol>(p, ws, ws_bytes, stream);
+    }
+}
+
+}  // namespace amx

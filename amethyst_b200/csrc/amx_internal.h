@@ -1,0 +1,89 @@
+// amx_internal.h -- definitions shared by the host launchers and the kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/amethyst.h"
+
+namespace amx {
+
+// Upper bound of every device-side spin (mbarrier phases, look-back flags).  Each spin
+// backs off with __nanosleep, so the bound is well above a second of waiting.
+constexpr uint32_t kWaitSpins = 1u << 20;
+
+// A column as the kernels see it.
+struct ColDev {
+    const void* data;
+    uint64_t n;
+    uint64_t bytes;  // storage bytes
+    uint64_t mask;   // mask(bits)
+    uint32_t format;
+    uint32_t bits;
+    uint32_t eps;  // elements per slab (slab format), else 0
+    uint32_t pad;
+};
+
+// Output column as the kernels see it.
+struct OutDev {
+    void* data;
+    uint64_t mask;
+    uint32_t format;
+    uint32_t bits;
+    uint32_t eps;
+    uint32_t pad;
+};
+
+// Workspace header, followed by one uint64 look-back status word per tile.
+struct WsHeader {
+    uint32_t ticket;  // next tile to hand out
+    uint32_t done;    // CTAs finished
+    uint32_t err;     // first device-side error (amx_status), 0 if none
+    uint32_t pad0;
+    unsigned long long count;  // survivors over all tiles
+    unsigned long long agg;    // encoded aggregate (identity 0)
+    uint64_t pad1[4];
+};
+static_assert(sizeof(WsHeader) == 64, "workspace header layout");
+
+constexpr uint32_t kFmtMask = 7;  // internal format tag of an input bitmask column
+constexpr uint32_t kPipeThreads = 256;
+constexpr uint32_t kStages = 2;
+
+// Parameters of the tile pipeline kernel (passed by value as a __grid_constant__).
+struct PipeParams {
+    ColDev a;
+    ColDev b;
+    ColDev m;  // optional input bitmask (format = AMX_PLAIN32, bits = 32), data NULL if none
+    OutDev out;
+    uint32_t has_b;
+    uint32_t has_mask_in;
+    uint32_t has_out;
+    uint32_t compact;  // 1: survivors are compacted (look-back); 0: element-wise map
+    uint32_t op;
+    uint32_t vbits;
+    uint64_t vmask;
+    uint64_t pred_lo;
+    uint64_t pred_span;
+    uint32_t pred_neg;
+    uint32_t has_pred;
+    uint32_t pred_lo32;   // 32-bit form of the predicate for values < 2^32 (pred32_ok)
+    uint32_t pred_span32;
+    uint32_t pred32_ok;
+    uint32_t pad2;
+    uint32_t agg;
+    uint32_t has_agg;
+    uint32_t* mask_out;
+    uint64_t* count_out;
+    uint64_t* agg_out;
+    WsHeader* ws;
+    uint64_t* status;
+    uint64_t n;
+    uint64_t num_tiles;
+    uint32_t tile_elems;
+    uint32_t stage_bytes;  // bytes of one pipeline stage (a | b | m buffers)
+    uint32_t a_off, b_off, m_off;  // offsets of the buffers inside a stage
+    uint32_t smem_fixed;           // bytes before the first stage
+};
+
+}  // namespace amx

@@ -1,0 +1,194 @@
+// amx_policies.cuh -- compile-time-width decode policies of the tile pipeline and the rule
+// that picks one for a request.
+//
+// A policy fixes R (elements per thread per tile) and decodes a thread's run of R elements
+// from the staged words.  GenericPol (amx_pipeline.cuh) handles any format and width with
+// runtime streaming readers.  The policies here fix the slab widths at compile time so
+// every shift and mask is a constant and each thread's run starts on a slab boundary:
+//   SlabPol<B>           one slab column of width B (filter, compressstore, reduce, convert)
+//   Slab2Pol<BA, BB>     two slab columns (binary op, fused chains)
+// Values are 32-bit, so these policies serve value widths up to 32.
+#pragma once
+
+#include "amx_pipeline.cuh"
+
+namespace amx {
+
+template <int A, int B>
+struct ct_gcd {
+    static constexpr int value = ct_gcd<B, A % B>::value;
+};
+template <int A>
+struct ct_gcd<A, 0> {
+    static constexpr int value = A;
+};
+
+// load N consecutive 64-bit words from shared memory, 16 bytes at a time when aligned
+template <int N>
+__device__ __forceinline__ void lds_words(const uint64_t* src, uint64_t (&w)[N])
+{
+    if constexpr (N % 2 == 0) {
+        const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+        for (int i = 0; i < N / 2; i++) {
+            const uint4 x = s[i];
+            w[2 * i] = ((uint64_t)x.y << 32) | x.x;
+            w[2 * i + 1] = ((uint64_t)x.w << 32) | x.z;
+        }
+    }
+    else {
+#pragma unroll
+        for (int i = 0; i < N; i++) w[i] = src[i];
+    }
+}
+
+template <int B, int K>
+__device__ __forceinline__ uint32_t field(uint64_t slab)
+{
+    return (uint32_t)((slab >> (K * B)) & ((1ull << B) - 1));
+}
+
+template <int B, int EPS, int N, int R>
+__device__ __forceinline__ void unpack_slabs(const uint64_t (&w)[N], uint32_t (&v)[R])
+{
+#pragma unroll
+    for (int j = 0; j < N; j++)
+#pragma unroll
+        for (int k = 0; k < EPS; k++) v[j * EPS + k] = (uint32_t)((w[j] >> (k * B)) & ((1ull << B) - 1));
+}
+
+// mask to the value width and evaluate the predicate on 32-bit values
+template <int R>
+__device__ __forceinline__ void finish32(const PipeParams& p, uint32_t (&v)[R], uint64_t& fl)
+{
+    if (p.vbits < 32) {
+        const uint32_t vm = (uint32_t)p.vmask;
+#pragma unroll
+        for (int i = 0; i < R; i++) v[i] &= vm;
+    }
+    if (!p.has_pred) {
+        fl = ~0ull;
+        return;
+    }
+    fl = 0;
+    if (p.pred32_ok) {
+        const uint32_t lo = p.pred_lo32, span = p.pred_span32;
+#pragma unroll
+        for (int i = 0; i < R; i++) fl |= (uint64_t)((v[i] - lo) <= span) << i;
+        if (p.pred_neg) fl = ~fl;
+    }
+    else {
+        const PredN pn{p.pred_lo, p.pred_span, p.pred_neg, 0};
+#pragma unroll
+        for (int i = 0; i < R; i++) fl |= (uint64_t)pred_eval(pn, (uint64_t)v[i]) << i;
+    }
+}
+
+template <int B>
+struct SlabPol {
+    using V = uint32_t;
+    static constexpr int EPS = 64 / B;
+    static constexpr int SPT = EPS >= 32 ? 1 : 32 / EPS;
+    static constexpr int R = EPS * SPT;
+
+    __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
+                                                  uint64_t first, V (&v)[R], uint64_t& fl)
+    {
+        const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first / EPS - sb[0] / 8);
+        uint64_t s[SPT];
+        lds_words<SPT>(w, s);
+        unpack_slabs<B, EPS, SPT, R>(s, v);
+        finish32<R>(p, v, fl);
+    }
+};
+
+template <int R>
+__device__ __forceinline__ void apply_op32(uint32_t op, uint32_t (&v)[R], const uint32_t (&r)[R])
+{
+    switch (op) {
+        case AMX_OP_ADD:
+#pragma unroll
+            for (int i = 0; i < R; i++) v[i] += r[i];
+            break;
+        case AMX_OP_SUB:
+#pragma unroll
+            for (int i = 0; i < R; i++) v[i] -= r[i];
+            break;
+        case AMX_OP_MUL:
+#pragma unroll
+            for (int i = 0; i < R; i++) v[i] *= r[i];
+            break;
+        default:
+#pragma unroll
+            for (int i = 0; i < R; i++) v[i] = (uint32_t)binop_eval(op, v[i], r[i]);
+            break;
+    }
+}
+
+template <int BA, int BB>
+struct Slab2Pol {
+    using V = uint32_t;
+    static constexpr int EA = 64 / BA;
+    static constexpr int EB = 64 / BB;
+    static constexpr int L = EA / ct_gcd<EA, EB>::value * EB;
+    static constexpr int R = L >= 32 ? L : L * (32 / L);
+    static constexpr int SA = R / EA;
+    static constexpr int SB = R / EB;
+    static_assert(R <= 64, "run too long for the flag word");
+
+    __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
+                                                  uint64_t first, V (&v)[R], uint64_t& fl)
+    {
+        {
+            const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first / EA - sb[0] / 8);
+            uint64_t s[SA];
+            lds_words<SA>(w, s);
+            unpack_slabs<BA, EA, SA, R>(s, v);
+        }
+        uint32_t r[R];
+        {
+            const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.b_off) + (first / EB - sb[1] / 8);
+            uint64_t s[SB];
+            lds_words<SB>(w, s);
+            unpack_slabs<BB, EB, SB, R>(s, r);
+        }
+        apply_op32<R>(p.op, v, r);
+        finish32<R>(p, v, fl);
+    }
+};
+
+// Policy ids: 0 generic, 1..32 SlabPol<B>, 100+ Slab2Pol pairs.
+#define AMX_SLAB2_PAIRS(X) X(100, 7, 13) X(101, 13, 7) X(102, 11, 11) X(103, 13, 13)
+
+#define AMX_POLICY_LIST(X)                                                                                             \
+    X(1, SlabPol<1>) X(2, SlabPol<2>) X(3, SlabPol<3>) X(4, SlabPol<4>) X(5, SlabPol<5>) X(6, SlabPol<6>)             \
+    X(7, SlabPol<7>) X(8, SlabPol<8>) X(9, SlabPol<9>) X(10, SlabPol<10>) X(11, SlabPol<11>) X(12, SlabPol<12>)       \
+    X(13, SlabPol<13>) X(14, SlabPol<14>) X(15, SlabPol<15>) X(16, SlabPol<16>) X(17, SlabPol<17>)                    \
+    X(18, SlabPol<18>) X(19, SlabPol<19>) X(20, SlabPol<20>) X(21, SlabPol<21>) X(22, SlabPol<22>)                    \
+    X(23, SlabPol<23>) X(24, SlabPol<24>) X(25, SlabPol<25>) X(26, SlabPol<26>) X(27, SlabPol<27>)                    \
+    X(28, SlabPol<28>) X(29, SlabPol<29>) X(30, SlabPol<30>) X(31, SlabPol<31>) X(32, SlabPol<32>)                    \
+    X(100, AMX_PAIR(7, 13)) X(101, AMX_PAIR(13, 7)) X(102, AMX_PAIR(11, 11)) X(103, AMX_PAIR(13, 13))
+#define AMX_PAIR(a, b) Slab2Pol<a, b>
+
+// Policy for a request: compile-time widths when every input is a slab column of width
+// <= 32 and values fit 32 bits, else the generic runtime-width policy.  `force` >= 0
+// selects a policy directly (the autotuner and the tests); an inapplicable force falls back
+// to the automatic choice.
+inline int choose_policy(const PipeParams& p, int force)
+{
+    const bool v32 = p.vbits <= 32;
+    const bool a_slab = p.a.format == AMX_SLAB && p.a.bits <= 32;
+    int auto_id = 0;
+    if (v32 && a_slab && !p.has_b) auto_id = (int)p.a.bits;
+    if (v32 && a_slab && p.has_b && p.b.format == AMX_SLAB) {
+#define AMX_PAIR_MATCH(id, x, y) \
+    if (p.a.bits == x && p.b.bits == y) auto_id = id;
+        AMX_SLAB2_PAIRS(AMX_PAIR_MATCH)
+#undef AMX_PAIR_MATCH
+    }
+    if (force == 0) return 0;
+    if (force > 0 && force == auto_id) return force;
+    return auto_id;
+}
+
+}  // namespace amx

@@ -1,0 +1,158 @@
+"""Python host mirror of the Amethyst operator layer, on top of the C ABI.
+
+Device buffers are torch tensors (torch is used for device memory and streams only); every
+operator call goes through libamethyst_b200.so.  These helpers allocate their outputs and
+workspaces with torch, which the C ABI itself never does.
+
+The operator names follow the reference's kernels and launchers (src/lib.cuh:4-46,
+src/kernels/*.cuh): filter, compressstore, binary_op, hop (= reduce), groupby, matmul.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _capi as A
+from ._capi import check, lib
+
+
+def _stream_ptr(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def storage_bytes(fmt: int, bits: int, n: int) -> int:
+    return int(lib().amx_storage_bytes(fmt, bits, n))
+
+
+def alloc_bytes(nbytes: int, device="cuda") -> torch.Tensor:
+    """A 16-byte-padded device byte buffer (torch allocations are 512-byte aligned)."""
+    return torch.zeros(max(16, (nbytes + 15) // 16 * 16 + 16), dtype=torch.uint8, device=device)
+
+
+@dataclass
+class PackedColumn:
+    """n elements of `bits` bits in `fmt`, stored in the byte tensor `data`."""
+    data: torch.Tensor
+    n: int
+    fmt: int
+    bits: int
+
+    @property
+    def desc(self) -> A.Column:
+        return A.Column(self.data.data_ptr(), self.n, self.fmt, self.bits)
+
+    @property
+    def nbytes(self) -> int:
+        return storage_bytes(self.fmt, self.bits, self.n)
+
+    @staticmethod
+    def empty(n: int, fmt: int, bits: int, device="cuda", capacity: int | None = None) -> "PackedColumn":
+        cap = n if capacity is None else capacity
+        return PackedColumn(alloc_bytes(storage_bytes(fmt, bits, cap), device), n, fmt, bits)
+
+    @staticmethod
+    def from_bytes(raw: bytes | memoryview, n: int, fmt: int, bits: int, device="cuda") -> "PackedColumn":
+        col = PackedColumn.empty(n, fmt, bits, device)
+        host = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+        col.data[: host.numel()].copy_(host)
+        return col
+
+    def host_bytes(self, n: int | None = None) -> bytes:
+        nb = storage_bytes(self.fmt, self.bits, self.n if n is None else n)
+        return self.data[:nb].cpu().numpy().tobytes()
+
+
+def predicate(kind: int, k0: int = 0, k1: int = 0, bits: int = 0) -> A.Predicate:
+    return A.Predicate(kind, bits, k0, k1)
+
+
+def workspace(n: int, device="cuda") -> torch.Tensor:
+    return torch.empty(int(lib().amx_workspace_bytes(n)), dtype=torch.uint8, device=device)
+
+
+def mask_words(n: int) -> int:
+    return (n + 31) // 32
+
+
+def filter(col: PackedColumn, pred: A.Predicate, ws=None, stream=None) -> torch.Tensor:
+    """Bitmask (int32 words, LSB-first) of pred over the column."""
+    mask = torch.zeros(mask_words(col.n) + 4, dtype=torch.int32, device=col.data.device)
+    ws = workspace(col.n, col.data.device) if ws is None else ws
+    check(lib().amx_filter(C.byref(col.desc), C.byref(pred), _ptr(mask), _ptr(ws), ws.numel(), _stream_ptr(stream)))
+    return mask
+
+
+def compressstore(col: PackedColumn, mask: torch.Tensor, out_fmt: int, out_bits: int, ws=None, stream=None):
+    """Survivors of the mask in order; returns (output column sized for n, count tensor)."""
+    out = PackedColumn.empty(col.n, out_fmt, out_bits, col.data.device)
+    cnt = torch.zeros(2, dtype=torch.int64, device=col.data.device)
+    ws = workspace(col.n, col.data.device) if ws is None else ws
+    check(lib().amx_compressstore(C.byref(col.desc), _ptr(mask), C.byref(out.desc), _ptr(cnt), _ptr(ws), ws.numel(),
+                                  _stream_ptr(stream)))
+    return out, cnt
+
+
+def filter_compressstore(col: PackedColumn, pred: A.Predicate, out_fmt: int, out_bits: int, ws=None, stream=None):
+    out = PackedColumn.empty(col.n, out_fmt, out_bits, col.data.device)
+    cnt = torch.zeros(2, dtype=torch.int64, device=col.data.device)
+    ws = workspace(col.n, col.data.device) if ws is None else ws
+    check(lib().amx_filter_compressstore(C.byref(col.desc), C.byref(pred), C.byref(out.desc), _ptr(cnt), _ptr(ws),
+                                         ws.numel(), _stream_ptr(stream)))
+    return out, cnt
+
+
+def binary_op(op: int, lhs: PackedColumn, rhs: PackedColumn, out_fmt: int, out_bits: int | None = None, ws=None,
+              stream=None) -> PackedColumn:
+    if out_bits is None:
+        out_bits = int(lib().amx_binary_out_bits(op, lhs.bits, rhs.bits))
+    out = PackedColumn.empty(lhs.n, out_fmt, out_bits, lhs.data.device)
+    ws = workspace(lhs.n, lhs.data.device) if ws is None else ws
+    check(lib().amx_binary(op, C.byref(lhs.desc), C.byref(rhs.desc), C.byref(out.desc), _ptr(ws), ws.numel(),
+                           _stream_ptr(stream)))
+    return out
+
+
+def convert(col: PackedColumn, out_fmt: int, out_bits: int, ws=None, stream=None) -> PackedColumn:
+    out = PackedColumn.empty(col.n, out_fmt, out_bits, col.data.device)
+    ws = workspace(col.n, col.data.device) if ws is None else ws
+    check(lib().amx_convert(C.byref(col.desc), C.byref(out.desc), _ptr(ws), ws.numel(), _stream_ptr(stream)))
+    return out
+
+
+def hop(agg: int, col: PackedColumn, mask: torch.Tensor | None = None, ws=None, stream=None) -> torch.Tensor:
+    """Aggregation into one uint64 (returned in an int64 tensor of one element)."""
+    res = torch.zeros(2, dtype=torch.int64, device=col.data.device)
+    ws = workspace(col.n, col.data.device) if ws is None else ws
+    check(lib().amx_reduce(agg, C.byref(col.desc), _ptr(mask), _ptr(res), _ptr(ws), ws.numel(), _stream_ptr(stream)))
+    return res[:1]
+
+
+reduce = hop
+
+
+def chain(lhs: PackedColumn, rhs: PackedColumn | None, op: int, value_bits: int, pred: A.Predicate,
+          agg: int = A.AGG_SUM, out_fmt: int | None = None, out_bits: int | None = None, want_mask: bool = False,
+          want_agg: bool = True, ws=None, stream=None):
+    """Fused v = op(lhs, rhs) -> filter pred(v) -> compressstore / mask / count / aggregate."""
+    dev = lhs.data.device
+    desc = A.ChainDesc(op, value_bits, pred, agg, 0)
+    out = PackedColumn.empty(lhs.n, out_fmt, out_bits or value_bits, dev) if out_fmt is not None else None
+    mask = torch.zeros(mask_words(lhs.n) + 4, dtype=torch.int32, device=dev) if want_mask else None
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    ag = torch.zeros(2, dtype=torch.int64, device=dev) if want_agg else None
+    ws = workspace(lhs.n, dev) if ws is None else ws
+    check(lib().amx_chain(C.byref(desc), C.byref(lhs.desc), C.byref(rhs.desc) if rhs is not None else None,
+                          C.byref(out.desc) if out is not None else None, _ptr(mask), _ptr(cnt), _ptr(ag), _ptr(ws),
+                          ws.numel(), _stream_ptr(stream)))
+    return out, mask, cnt, ag
+
+
+def workspace_status(ws: torch.Tensor, stream=None) -> None:
+    check(lib().amx_workspace_status(_ptr(ws), _stream_ptr(stream)))

@@ -1,0 +1,188 @@
+/*
+ * amethyst.h -- C ABI of the B200-native Amethyst operator layer (libamethyst_b200.so).
+ *
+ * Every operator accepts columns in any storage format and writes any storage format:
+ *
+ *   AMX_PLAIN32  one uint32 per element, value = word & mask(bits), bits 1..32
+ *   AMX_PLAIN64  one uint64 per element, value = word & mask(bits), bits 1..64
+ *                (the reference's "baseline" format: src/common_code.cuh:51-55)
+ *   AMX_SLAB     floor(64/bits) elements per little-endian uint64 slab, element i in slab
+ *                i/eps at bit (i%eps)*bits, dead top bits ignored on read and written 0
+ *                (the reference's "slabs" format: src/common_code.cuh:43-50)
+ *   AMX_NOGAPS   continuous bit stream, element i at bit i*bits
+ *                (the reference's "nogaps" format: src/common_code.cuh:100-116)
+ *
+ * Bitmasks are LSB-first bit arrays in uint32 words (bit i of the mask = bit i%32 of word
+ * i/32), bits past n zero -- the layout the reference's filter writes
+ * (src/kernels/filter_slabs.cuh:55) and its compressstore reads (src/bit_iterator.cuh:18-21).
+ *
+ * Conventions shared by every entry point:
+ *   - all data pointers are device pointers aligned to 16 bytes (cudaMalloc gives 256);
+ *   - calls are asynchronous on `stream` (a cudaStream_t; NULL = legacy default stream),
+ *     never synchronise, and never allocate memory;
+ *   - operators that need scratch memory take a caller-owned device workspace of at least
+ *     amx_workspace_bytes(n) bytes; the call clears the part it uses with
+ *     cudaMemsetAsync on `stream`.  A workspace must not be shared by calls that may
+ *     overlap on the GPU;
+ *   - results that are scalars (counts, aggregates, group counts) are written to device
+ *     memory, so a sequence of calls can be captured into a CUDA graph;
+ *   - device-side failures (a bounded wait that ran out) are recorded in the workspace and
+ *     read back with amx_workspace_status(), which synchronises the stream.
+ * The status codes replace the reference's print-and-exit error handling
+ * (src/cuda_try.cuh:8-21).
+ */
+#ifndef AMETHYST_H
+#define AMETHYST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMX_VERSION 100
+
+typedef enum {
+    AMX_OK = 0,
+    AMX_ERR_INVALID_ARG = 1,  /* null pointer, bad width, size mismatch, unknown enum */
+    AMX_ERR_UNSUPPORTED = 2,  /* valid request this build does not implement */
+    AMX_ERR_ALIGNMENT = 3,    /* a data pointer is not 16-byte aligned */
+    AMX_ERR_WORKSPACE = 4,    /* workspace missing or smaller than required */
+    AMX_ERR_CUDA = 5,         /* a CUDA runtime call failed (see amx_last_error) */
+    AMX_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up; outputs are invalid */
+    AMX_ERR_CAPACITY = 7      /* a size exceeds a documented maximum */
+} amx_status;
+
+typedef enum { AMX_PLAIN32 = 0, AMX_PLAIN64 = 1, AMX_SLAB = 2, AMX_NOGAPS = 3 } amx_format;
+
+/* A column: `n` elements of `bits` bits stored at `data` in `format`. */
+typedef struct {
+    void* data;
+    uint64_t n;
+    uint32_t format;
+    uint32_t bits;
+} amx_column;
+
+/* Predicates.  The reference compiles one predicate into each kernel instance
+ * (FILTER_PREDICATE_OP, src/config.cuh:107-113); here it is a runtime descriptor.
+ * AMX_PRED_HALF is that reference predicate: v >= 2^(bits-1), `bits` taken from the
+ * descriptor. */
+typedef enum {
+    AMX_PRED_ALL = 0,
+    AMX_PRED_LT = 1,          /* v <  k0 */
+    AMX_PRED_LE = 2,          /* v <= k0 */
+    AMX_PRED_GT = 3,          /* v >  k0 */
+    AMX_PRED_GE = 4,          /* v >= k0 */
+    AMX_PRED_EQ = 5,          /* v == k0 */
+    AMX_PRED_NE = 6,          /* v != k0 */
+    AMX_PRED_BETWEEN = 7,     /* k0 <= v <= k1 */
+    AMX_PRED_NOT_BETWEEN = 8, /* !(k0 <= v <= k1) */
+    AMX_PRED_HALF = 9         /* v >= 2^(bits-1) */
+} amx_pred_kind;
+
+typedef struct {
+    uint32_t kind;
+    uint32_t bits;
+    uint64_t k0;
+    uint64_t k1;
+} amx_predicate;
+
+/* Element-wise binary operators; every result is masked to the output column's width like
+ * the reference's op_* templates (src/config.cuh:5-42).  x/0 = all ones, x%0 = x. */
+typedef enum {
+    AMX_OP_ADD = 0,
+    AMX_OP_SUB = 1,      /* (l - r) mod 2^out_bits */
+    AMX_OP_MUL = 2,
+    AMX_OP_DIV = 3,
+    AMX_OP_MOD = 4,
+    AMX_OP_MIN = 5,
+    AMX_OP_MAX = 6,
+    AMX_OP_AND = 7,
+    AMX_OP_OR = 8,
+    AMX_OP_XOR = 9,
+    AMX_OP_BOOL_OR = 10,  /* op_bool_simple  */
+    AMX_OP_BOOL_XOR = 11, /* op_bool_complex */
+    AMX_OP_MATH = 12,     /* op_math: (l*l + r*r + 4l) / (l*l + r*r + 5l) */
+    AMX_OP_LHS = 13       /* identity on the left operand */
+} amx_binop;
+
+/* Horizontal aggregations ("hop", src/config.cuh:62-71), all into uint64. */
+typedef enum { AMX_AGG_SUM = 0, AMX_AGG_MIN = 1, AMX_AGG_MAX = 2, AMX_AGG_AND = 3, AMX_AGG_OR = 4, AMX_AGG_XOR = 5 } amx_agg;
+
+/* ---- sizing and diagnostics --------------------------------------------------------- */
+int amx_version(void);
+const char* amx_status_string(amx_status s);
+/* message of the last failed call on this host thread */
+const char* amx_last_error(void);
+/* storage bytes of a column of n elements */
+uint64_t amx_storage_bytes(uint32_t format, uint32_t bits, uint64_t n);
+/* bytes of an n-element bitmask: ceil(n/32) * 4 */
+uint64_t amx_mask_bytes(uint64_t n);
+/* narrowest output width that never truncates op(lhs, rhs) */
+uint32_t amx_binary_out_bits(uint32_t op, uint32_t lhs_bits, uint32_t rhs_bits);
+/* workspace bytes needed by the column operators on n elements */
+uint64_t amx_workspace_bytes(uint64_t n);
+/* synchronises `stream`, then reports a device-side failure recorded in `workspace` by the
+ * last call that used it (AMX_OK if none) */
+amx_status amx_workspace_status(const void* workspace, void* stream);
+
+/* ---- column operators ------------------------------------------------------------------ */
+
+/* filter -> bitmask.  Replaces kernel_filter_{slabs,nogaps,baseline}
+ * (src/kernels/filter_slabs.cuh:4-57, filter_nogaps.cuh:4-65, filter_baseline.cuh:9-36). */
+amx_status amx_filter(const amx_column* in, const amx_predicate* pred, uint32_t* d_mask, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/* compressstore: the elements whose mask bit is set, in order, written to `out`
+ * (out->n is its capacity and must be >= in->n); the survivor count goes to *d_count.
+ * Replaces the popcount -> scan -> write pipeline of bench_compressstore_slabs
+ * (src/benchs/bench_compressstore_slabs.cu:38-56, kernels
+ * src/kernels/compressstore_slabs.cuh:4-206) and the CUB plain path
+ * (src/benchs/bench_compressstore_baseline_cub.cu:35). */
+amx_status amx_compressstore(const amx_column* in, const uint32_t* d_mask, const amx_column* out, uint64_t* d_count,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* filter fused with compressstore: no mask is materialised. */
+amx_status amx_filter_compressstore(const amx_column* in, const amx_predicate* pred, const amx_column* out,
+                                    uint64_t* d_count, void* workspace, size_t workspace_bytes, void* stream);
+
+/* element-wise binary op, lhs and rhs may differ in format and width.  Replaces
+ * kernel_binary_op_{slabs,nogaps,baseline} (src/kernels/binary_op_slabs.cuh:7-67,
+ * binary_op_nogaps.cuh:5-89, binary_op_baseline.cuh:4-13). */
+amx_status amx_binary(uint32_t op, const amx_column* lhs, const amx_column* rhs, const amx_column* out,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* re-encode a column in another format / width (values masked to out->bits). */
+amx_status amx_convert(const amx_column* in, const amx_column* out, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* aggregation of all elements (d_mask NULL) or of the masked ones.  Replaces
+ * kernel_hop_{slabs,nogaps} (src/kernels/hop.cuh:7-76) and cub::DeviceReduce
+ * (src/benchs/bench_hop_baseline_cub.cu:38). */
+amx_status amx_reduce(uint32_t agg, const amx_column* in, const uint32_t* d_mask, uint64_t* d_result,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- fused operator chain -------------------------------------------------------------- */
+/* v = op(lhs, rhs) masked to value_bits (v = lhs when rhs is NULL), keep the elements with
+ * pred(v), then any of: the survivors compacted into `out`, the bitmask of pred(v) into
+ * d_mask, the survivor count into *d_count, agg over the survivors into *d_agg.  Each
+ * output pointer may be NULL.  One pass over the inputs; no intermediate reaches memory.
+ * The reference has no fused chain (src/op_chaining_demo.cu:137-152 runs operators one
+ * after another). */
+typedef struct {
+    uint32_t op;
+    uint32_t value_bits;
+    amx_predicate pred;
+    uint32_t agg;
+    uint32_t reserved;
+} amx_chain_desc;
+
+amx_status amx_chain(const amx_chain_desc* desc, const amx_column* lhs, const amx_column* rhs, const amx_column* out,
+                     uint32_t* d_mask, uint64_t* d_count, uint64_t* d_agg, void* workspace, size_t workspace_bytes,
+                     void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

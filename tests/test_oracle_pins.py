@@ -1,0 +1,83 @@
+"""The C oracle against the reference's own host code run live (oracle/_ref/libamxref_host.so),
+on fresh random inputs, plus the oracle's own algebraic consistency.  Skipped where the
+reference could not be built (the GPU machine has no reference tree)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+@pytest.fixture(scope="module")
+def ref():
+    h = O.ref_host()
+    if h is None:
+        try:
+            O.build(with_reference=True)
+        except Exception:
+            pass
+        h = O.ref_host()
+    if h is None:
+        pytest.skip("reference host code not built (no reference tree)")
+    return h
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_accessors_live(ref, seed):
+    rng = np.random.default_rng(seed)
+    words = rng.integers(0, 2**63, size=64, dtype=np.uint64) * np.uint64(2) + np.uint64(seed & 1)
+    raw = np.concatenate([words, np.zeros(4, np.uint64)]).view(np.uint8)
+    for b in range(1, 65):
+        n_slab = 64 * (64 // b)
+        vals = O.decode(raw, n_slab, O.SLAB, b)
+        for i in rng.choice(n_slab, size=min(n_slab, 40), replace=False):
+            assert vals[i] == ref.amxref_get_element(b, O._p(words), int(i))
+        n_ng = (63 * 64) // b
+        vals = O.decode(raw, n_ng, O.NOGAPS, b)
+        for i in rng.choice(n_ng, size=min(n_ng, 40), replace=False):
+            assert vals[i] == ref.amxref_get_elem_nogaps(b, O._p(words), int(i))
+        vals = O.decode(raw, 64, O.PLAIN64, b)
+        for i in range(0, 64, 5):
+            assert vals[i] == ref.amxref_get_element_baseline(b, O._p(words), i)
+
+
+def test_operators_live(ref):
+    rng = np.random.default_rng(7)
+    for _ in range(400):
+        ob = int(rng.integers(1, 65))
+        lb = int(rng.integers(1, 33))
+        lv = int(rng.integers(1, 1 << lb))
+        rv = int(rng.integers(1, 1 << lb))
+        for op in (0, 2, 3, 4, 10, 11, 12):
+            assert O.ora().ora_binop(op, lv, rv, ob) == ref.amxref_op(op, ob, lv, rv), (op, ob, lv, rv)
+
+
+def test_main_inputs_and_masks_live(ref):
+    n = 1 << 14
+    ok, d1, d2 = O.run_reference_main(["-n", str(n), "--nv"], n)
+    assert ok
+    e1, e2 = O.reference_inputs(42, n)
+    assert np.array_equal(d1, e1) and np.array_equal(d2, e2)
+    ok, _, m = O.run_reference_main(["-n", str(n), "--nv", "-m", "2", "-s", "0.25"], n)
+    assert np.array_equal(m.view(np.uint8)[: n // 8], O.mask_clusters(0.25, 8, n))
+
+
+def test_encode_decode_roundtrip():
+    for fmt in (O.PLAIN32, O.PLAIN64, O.SLAB, O.NOGAPS):
+        for b in ([1, 5, 11, 17, 31, 32] + ([] if fmt == O.PLAIN32 else [33, 50, 63, 64])):
+            for n in (0, 1, 63, 64, 65, 1000):
+                v = O.uniform_values(b * 1000 + n, b, n)
+                raw = O.encode(fmt, b, v)
+                assert np.array_equal(O.decode(raw, n, fmt, b), v)
+
+
+def test_compressstore_is_filter_then_select():
+    n = 5000
+    v = O.uniform_values(3, 11, n)
+    raw = O.encode(O.SLAB, 11, v)
+    p = O.pred(1, 205)
+    mask = O.filter(raw, n, O.SLAB, 11, p)
+    out1, c1 = O.compressstore(raw, n, O.SLAB, 11, mask, O.SLAB, 11)
+    out2, c2 = O.filter_compressstore(raw, n, O.SLAB, 11, p, O.SLAB, 11)
+    assert c1 == c2 == int((v < 205).sum())
+    assert np.array_equal(out1, out2)
+    assert np.array_equal(O.decode(out1, c1, O.SLAB, 11), v[v < 205])
