@@ -77,6 +77,7 @@ ColDev col_dev(const amx_column* c)
     d.format = c->format;
     d.bits = c->bits;
     d.eps = c->format == AMX_SLAB ? 64 / c->bits : 0;
+    d.magic = d.eps >= 2 ? (uint32_t)((1ull << 32) / d.eps + 1) : 0;
     return d;
 }
 

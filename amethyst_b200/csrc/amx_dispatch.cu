@@ -44,7 +44,9 @@ static amx_status launch(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t 
     p.m_off = off;
     if (p.has_mask_in) off += stage_need(p.m, TILE);
     p.stage_bytes = off;
-    p.smem_fixed = p.has_out ? round_up(kCvOff + TILE * (uint32_t)sizeof(typename Pol::V), 128) : kCvOff;
+    using V = typename Pol::V;
+    const uint32_t cv_entries = TILE + TILE / (sizeof(V) == 4 ? 32 : 16) + 1;  // bank skew padding
+    p.smem_fixed = p.has_out ? round_up(kCvOff + cv_entries * (uint32_t)sizeof(V), 128) : kCvOff;
     const uint32_t smem = p.smem_fixed + kStages * p.stage_bytes;
     if (smem > 227 * 1024) return fail(AMX_ERR_UNSUPPORTED, "pipeline needs %u bytes of shared memory", smem);
 

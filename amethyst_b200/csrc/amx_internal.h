@@ -20,8 +20,8 @@ struct ColDev {
     uint64_t mask;   // mask(bits)
     uint32_t format;
     uint32_t bits;
-    uint32_t eps;  // elements per slab (slab format), else 0
-    uint32_t pad;
+    uint32_t eps;    // elements per slab (slab format), else 0
+    uint32_t magic;  // floor(2^32 / eps) + 1 for eps >= 2: x / eps == umulhi(x, magic) for x < 2^17
 };
 
 // Output column as the kernels see it.

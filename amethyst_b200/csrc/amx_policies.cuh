@@ -90,10 +90,12 @@ struct SlabPol {
     static constexpr int EPS = 64 / B;
     static constexpr int SPT = EPS >= 32 ? 1 : 32 / EPS;
     static constexpr int R = EPS * SPT;
+    static constexpr bool kWarpMajor = false;
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
-                                                  uint64_t first, V (&v)[R], uint64_t& fl)
+                                                  uint64_t e0, V (&v)[R], uint64_t& fl)
     {
+        const uint64_t first = e0 + threadIdx.x * R;
         const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first / EPS - sb[0] / 8);
         uint64_t s[SPT];
         lds_words<SPT>(w, s);
@@ -134,11 +136,13 @@ struct Slab2Pol {
     static constexpr int R = L >= 32 ? L : L * (32 / L);
     static constexpr int SA = R / EA;
     static constexpr int SB = R / EB;
+    static constexpr bool kWarpMajor = false;
     static_assert(R <= 64, "run too long for the flag word");
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
-                                                  uint64_t first, V (&v)[R], uint64_t& fl)
+                                                  uint64_t e0, V (&v)[R], uint64_t& fl)
     {
+        const uint64_t first = e0 + threadIdx.x * R;
         {
             const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first / EA - sb[0] / 8);
             uint64_t s[SA];

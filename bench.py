@@ -1,0 +1,437 @@
+"""Benchmark of the Amethyst B200 operator layer.
+
+Default workload (the operator-chain configuration, one step = one pass):
+  A: 2^26 uint32 values uniform in [0, 2^7), packed in 7-bit slabs;
+  B: 2^26 uint32 values uniform in [0, 2^13), packed in 13-bit slabs;
+  C = A + B at 14 bits, keep C >= 2^13, compressstore the survivors as 14-bit slabs, and sum
+  them into a uint64 -- one fused pass (amx_chain) through the C ABI.
+`value` is packed GB/s = algorithmic bytes (packed inputs + packed output + scalars) / time,
+with inputs resident in HBM (194.9 MB > 126 MB L2, so no flush is needed between steps).
+`e2e` is the same metric through the same call with pinned host buffers, the host->device
+copy of the inputs and the device->host copy of the results inside the timed region.
+
+--impl reference runs the CPU arm: the scalar C oracle (a restatement of the reference's
+accessors and operators; the reference itself has no CPU implementation of the path) on all
+host cores over the same workload.
+
+Multi-GPU (torchrun): every rank runs its own copy of the workload on its own GPU (the path
+has no exchange step); value = all ranks' bytes / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "packed-op GB/s & % HBM peak; batched+learned-format vs plain, 1 B200, bit-exact"
+N_CHAIN = 1 << 26
+BITS_A, BITS_B, BITS_C = 7, 13, 14
+THRESH = 1 << 13
+SEED_A, SEED_B = 0x5EED_A, 0x5EED_B
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def storage_bytes(fmt, bits, n):
+    if fmt == 0:
+        return 4 * n
+    if fmt == 1:
+        return 8 * n
+    if fmt == 2:
+        eps = 64 // bits
+        return 8 * ((n + eps - 1) // eps)
+    return 8 * ((n * bits + 63) // 64)
+
+
+# ------------------------------------------------------------------------------------------
+# clocks during the timed region (NVML reads only)
+# ------------------------------------------------------------------------------------------
+class ClockSampler:
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.stop_flag = [], 0, False
+        self.ok = False
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _sample(self):
+        try:
+            self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            try:
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                r = self.nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+            self.reasons |= int(r) & ~0x1
+        except Exception:
+            pass
+
+    def _run(self):
+        while not self.stop_flag:
+            self._sample()
+            time.sleep(0.01)
+
+    def start(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+
+    def stop(self):
+        if self.ok:
+            self.stop_flag = True
+            self.t.join()
+            self._sample()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": [v for k, v in self.REASONS.items() if self.reasons & k], "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------
+def pack_gpu(n, bits, seed, fmt):
+    """Generate uniform values on the GPU and encode them with amx_convert."""
+    from amethyst_b200 import datagen, ops
+
+    plain = datagen.uniform_gpu(n, bits, seed)
+    src = ops.PackedColumn(plain.view(__import__("torch").uint8), n, 0, 32)
+    return ops.convert(src, fmt, bits)
+
+
+def time_steps(fn, steps, warmup, stream):
+    """W warm-up calls, then exactly `steps` timed calls with an event pair around each one."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for a, b in evs:
+        a.record(stream)
+        fn()
+        b.record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    per = [a.elapsed_time(b) for a, b in evs]
+    return total_ms, per
+
+
+def chain_workload(dev, out_fmt=2, a_fmt=2, b_fmt=2, thresh=THRESH):
+    """Build the chain inputs and return (step function, algorithmic bytes fn, state)."""
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = N_CHAIN
+    a = pack_gpu(n, BITS_A, SEED_A, a_fmt)
+    b = pack_gpu(n, BITS_B, SEED_B, b_fmt)
+    out = ops.PackedColumn.empty(n, out_fmt, BITS_C)
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    agg = torch.zeros(2, dtype=torch.int64, device=dev)
+    ws = ops.workspace(n)
+    pred = ops.predicate(A.PRED_GE, thresh, 0, BITS_C)
+    desc = A.ChainDesc(A.OP_ADD, BITS_C, pred, A.AGG_SUM, 0)
+    import ctypes as C
+
+    L = A.lib()
+    a_d, b_d, o_d = a.desc, b.desc, out.desc
+    args = (C.byref(desc), C.byref(a_d), C.byref(b_d), C.byref(o_d), None, C.c_void_p(cnt.data_ptr()),
+            C.c_void_p(agg.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel())
+    state = {"a": a, "b": b, "out": out, "cnt": cnt, "agg": agg, "ws": ws, "desc": desc, "n": n}
+
+    def step(stream_ptr=None):
+        s = C.c_void_p(torch.cuda.current_stream().cuda_stream) if stream_ptr is None else stream_ptr
+        A.check(L.amx_chain(*args, s))
+
+    in_bytes = storage_bytes(a_fmt, BITS_A, n) + storage_bytes(b_fmt, BITS_B, n)
+
+    def alg_bytes(count):
+        return in_bytes + storage_bytes(out_fmt, BITS_C, count) + 16
+
+    return step, alg_bytes, state, in_bytes
+
+
+def e2e_chain(dev, steps, warmup):
+    """amx_chain through the C ABI with pinned host buffers: H2D inputs, chain, D2H results."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+
+    step, alg_bytes, st, in_bytes = chain_workload(dev)
+    a, b, out = st["a"], st["b"], st["out"]
+    ha = torch.empty(a.data.numel(), dtype=torch.uint8, pin_memory=True)
+    hb = torch.empty(b.data.numel(), dtype=torch.uint8, pin_memory=True)
+    ha.copy_(a.data)
+    hb.copy_(b.data)
+    hout = torch.empty(out.data.numel(), dtype=torch.uint8, pin_memory=True)
+    hres = torch.empty(4, dtype=torch.int64, pin_memory=True)
+    stream = torch.cuda.current_stream()
+    d2h = [0]
+
+    def e2e_step():
+        a.data.copy_(ha, non_blocking=True)
+        b.data.copy_(hb, non_blocking=True)
+        step()
+        hres[:2].copy_(st["cnt"], non_blocking=True)
+        hres[2:].copy_(st["agg"], non_blocking=True)
+        stream.synchronize()
+        c = int(hres[0])
+        nb = storage_bytes(2, BITS_C, c)
+        hout[:nb].copy_(out.data[:nb], non_blocking=True)
+        stream.synchronize()
+        d2h[0] = nb + 16
+
+    for _ in range(warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    c = int(hres[0])
+    return {"value": alg_bytes(c) / dt / 1e9, "unit": "GB/s", "h2d_bytes_per_step": in_bytes,
+            "d2h_bytes_per_step": d2h[0], "ms_per_step": dt * 1e3}
+
+
+def fc_1gib(dev, steps, warmup):
+    """The north-star column: 1 GiB of 11-bit slabs (2^27 slabs, 671,088,640 elements),
+    fused filter v < 205 + compressstore into 11-bit slabs."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = (1 << 27) * 5
+    col = pack_gpu(n, 11, 0xC0FFEE, 2)
+    out = ops.PackedColumn.empty(n, 2, 11)
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    ws = ops.workspace(n)
+    pred = ops.predicate(A.PRED_LT, 205, 0, 11)
+    L = A.lib()
+    cd, od = col.desc, out.desc
+
+    def step():
+        A.check(L.amx_filter_compressstore(C.byref(cd), C.byref(pred), C.byref(od), C.c_void_p(cnt.data_ptr()),
+                                           C.c_void_p(ws.data_ptr()), ws.numel(),
+                                           C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    total, per = time_steps(step, steps, warmup, torch.cuda.current_stream())
+    c = int(cnt[0].item())
+    byts = storage_bytes(2, 11, n) + storage_bytes(2, 11, c) + 8
+    ms = total / steps
+    del col, out, ws
+    torch.cuda.empty_cache()
+    return {"workload": "filter v<205 + compressstore, 1 GiB column of 11-bit slabs (671,088,640 elements)",
+            "GB_s": byts / (ms * 1e-3) / 1e9, "ms_per_step": ms, "selectivity": c / n, "alg_bytes": byts}
+
+
+def cpu_baseline_chain(st, threads):
+    """The C oracle (scalar restatement of the reference semantics) on the host cores over the
+    same packed inputs: count + sum of the chain; also checks the GPU result."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    n = st["n"]
+    araw = st["a"].data.cpu().numpy()
+    braw = st["b"].data.cpu().numpy()
+    p = O.pred(4, THRESH)
+    t0 = time.perf_counter()
+    cnt, agg = O.chain_mt(0, (araw, 2, BITS_A), (braw, 2, BITS_B), BITS_C, p, 0, n, threads)
+    dt = time.perf_counter() - t0
+    gc = int(st["cnt"][0].item())
+    ga = int(st["agg"].cpu().numpy().view(np.uint64)[0])
+    in_bytes = storage_bytes(2, BITS_A, n) + storage_bytes(2, BITS_B, n)
+    return dt, cnt, agg, (gc == cnt and ga == agg), in_bytes
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from amethyst_b200 import build as B
+
+    if not os.path.exists(B.LIB):
+        B.build()
+
+    step, alg_bytes, st, in_bytes = chain_workload(dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    total_ms, per = time_steps(step, args.steps, 0, stream)
+    sampler.stop()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    count = int(st["cnt"][0].item())
+    ms = total_ms / args.steps
+    byts = alg_bytes(count)
+    value = world * byts / (ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    kern_ms = statistics.mean(per)
+    achieved = byts / (kern_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("chain_7_13_to_14_slab")
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "operator chain at 256 MB: A u7 slab + B u13 slab -> C 14 bits, filter C >= 2^13, "
+                               "compressstore to 14-bit slabs, sum to uint64 (one fused pass)",
+                   "elements": N_CHAIN, "input_bytes": in_bytes, "survivors": count,
+                   "selectivity": count / N_CHAIN, "l2": "inputs (194.9 MB) larger than L2, no flush",
+                   "parallelism": f"replicas x{world}"},
+        "hbm_frac": round(byts / (ms * 1e-3) / 1e9 / peak, 4),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "amx::pipe_kernel<Slab2Pol<7,13>>", "alg_bytes_per_launch": byts,
+                     "launch_ms": round(kern_ms, 5)},
+        "gpu_launches": args.steps,
+        "clocks": sampler.summary(),
+    }
+    if rank == 0:
+        # end to end through the same C ABI call with host buffers
+        line["e2e"] = e2e_chain(dev, steps=max(3, min(args.steps, 20)), warmup=2)
+        if world == 1 and not args.no_extra:
+            extra = {}
+            try:
+                extra["fc_1gib"] = fc_1gib(dev, steps=max(3, min(args.steps, 30)), warmup=3)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["fc_1gib"] = {"error": str(e)}
+            for name, kw in [("chain_50pct", {"thresh": 4160}), ("chain_plain32_in", {"a_fmt": 0, "b_fmt": 0}),
+                             ("chain_plain32_out", {"out_fmt": 0})]:
+                s2, ab2, st2, ib2 = chain_workload(dev, **kw)
+                tot2, per2 = time_steps(s2, max(3, min(args.steps, 50)), 3, stream)
+                c2 = int(st2["cnt"][0].item())
+                ms2 = tot2 / max(3, min(args.steps, 50))
+                extra[name] = {"GB_s": round(ab2(c2) / (ms2 * 1e-3) / 1e9, 2), "ms_per_step": round(ms2, 5),
+                               "selectivity": c2 / N_CHAIN, "alg_bytes": ab2(c2)}
+                del s2, st2
+            line["extra"] = extra
+        if world == 1:
+            threads = len(os.sched_getaffinity(0))
+            dt, ccnt, cagg, ok, ib = cpu_baseline_chain(st, threads)
+            line["cpu_baseline"] = {"value": round((ib + storage_bytes(2, BITS_C, ccnt) + 16) / dt / 1e9, 3),
+                                    "unit": "GB/s", "cores": threads, "kind": "port",
+                                    "sample": "the full chain workload once (count + sum; the C oracle)",
+                                    "seconds": round(dt, 3), "matches_gpu": ok}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------
+# reference (CPU) arm
+# ------------------------------------------------------------------------------------------
+def run_reference(args):
+    import numpy as np
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from amethyst_b200 import datagen
+    from oracle import oracle as O
+
+    n = N_CHAIN
+    a = O.encode(2, BITS_A, datagen.uniform_np(SEED_A, BITS_A, n))
+    b = O.encode(2, BITS_B, datagen.uniform_np(SEED_B, BITS_B, n))
+    threads = len(os.sched_getaffinity(0))
+    p = O.pred(4, THRESH)
+    for _ in range(max(1, args.warmup)):
+        O.chain_mt(0, (a, 2, BITS_A), (b, 2, BITS_B), BITS_C, p, 0, n, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cnt, agg = O.chain_mt(0, (a, 2, BITS_A), (b, 2, BITS_B), BITS_C, p, 0, n, threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    byts = storage_bytes(2, BITS_A, n) + storage_bytes(2, BITS_B, n) + storage_bytes(2, BITS_C, cnt) + 16
+    v = byts / dt / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "operator chain at 256 MB: A u7 slab + B u13 slab -> C 14 bits, filter C >= 2^13, "
+                                   "compressstore to 14-bit slabs, sum to uint64", "elements": n, "survivors": cnt},
+            "cpu_baseline": {"value": round(v, 3), "unit": "GB/s", "cores": threads, "kind": "port",
+                             "sample": "the full chain workload per step (count + sum; the C oracle, which restates "
+                                       "the reference's accessors and operators)"},
+            "e2e": {"value": round(v, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="amethyst", choices=["amethyst", "reference"])
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

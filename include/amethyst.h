@@ -182,6 +182,15 @@ amx_status amx_chain(const amx_chain_desc* desc, const amx_column* lhs, const am
                      uint32_t* d_mask, uint64_t* d_count, uint64_t* d_agg, void* workspace, size_t workspace_bytes,
                      void* stream);
 
+/* ---- synthetic data (benchmarks and tests; no reference counterpart) --------------------- */
+/* element i = top `bits` bits of splitmix64(seed + (i+1)*0x9E3779B97F4A7C15) followed by one
+ * xorshift64 (13,7,17) step, written as plain uint32 (elem_bytes 4) or uint64 (8) words */
+amx_status amx_fill_uniform(void* d_out, uint64_t n, uint32_t elem_bytes, uint32_t bits, uint64_t seed, void* stream);
+/* keys by inverse CDF: u = draw(i) >> 11 scaled to [0,1), key = first k with d_cdf[k] > u
+ * (d_cdf: `groups` ascending doubles ending at 1.0) -- e.g. Zipf-distributed group keys */
+amx_status amx_fill_from_cdf(uint32_t* d_out, uint64_t n, const double* d_cdf, uint32_t groups, uint64_t seed,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif
