@@ -147,6 +147,17 @@ amx_status amx_compressstore(const amx_column* in, const uint32_t* d_mask, const
 amx_status amx_filter_compressstore(const amx_column* in, const amx_predicate* pred, const amx_column* out,
                                     uint64_t* d_count, void* workspace, size_t workspace_bytes, void* stream);
 
+/* filter fused with compressstore for callers that cannot allocate device memory (no
+ * counterpart in the reference).  Identical results to amx_filter_compressstore, but it takes no
+ * workspace: its scratch is a fixed 1 MiB array inside the library's device memory, held by
+ * every GPU that loads the library until the process exits.  Columns longer than 2^29 elements
+ * are rejected with AMX_ERR_CAPACITY.  All calls share that array and each call clears what it
+ * needs first, so calls ordered on one stream are fine but calls that may overlap on the GPU
+ * race.  The first call on a device looks up the array's address there; make it before any
+ * stream capture starts.  Calls no cudaMalloc, cudaFree or allocating library routine. */
+amx_status amx_filter_compressstore_noalloc(const amx_column* in, const amx_predicate* pred, const amx_column* out,
+                                            uint64_t* d_count, void* stream);
+
 /* element-wise binary op, lhs and rhs may differ in format and width.  Replaces
  * kernel_binary_op_{slabs,nogaps,baseline} (src/kernels/binary_op_slabs.cuh:7-67,
  * binary_op_nogaps.cuh:5-89, binary_op_baseline.cuh:4-13). */
