@@ -59,6 +59,8 @@ _SIGS = {
     "amx_convert": (C.c_int, [_COL, _COL, _P, C.c_size_t, _P]),
     "amx_reduce": (C.c_int, [C.c_uint32, _COL, _P, _P, _P, C.c_size_t, _P]),
     "amx_chain": (C.c_int, [C.POINTER(ChainDesc), _COL, _COL, _COL, _P, _P, _P, _P, C.c_size_t, _P]),
+    "amx_groupby_workspace_bytes": (C.c_uint64, [C.c_uint32]),
+    "amx_groupby": (C.c_int, [_COL, _COL, _P, _COL, _COL, _COL, _P, _P, C.c_size_t, _P]),
     "amx_fill_uniform": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _P]),
     "amx_fill_from_cdf": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P]),
 }

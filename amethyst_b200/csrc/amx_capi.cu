@@ -29,6 +29,9 @@ amx_status cuda_fail(cudaError_t e, const char* what)
 
 uint64_t mask_of(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1); }
 
+// floor(2^64 / d) + 1 for 2 <= d <= 64 (0 otherwise): exact n / d = umul64hi(n, m) for n < 2^58
+uint64_t magic64(uint32_t d) { return d >= 2 ? (uint64_t)(((unsigned __int128)1 << 64) / d) + 1 : 0; }
+
 uint64_t storage_bytes(uint32_t format, uint32_t bits, uint64_t n)
 {
     switch (format) {
@@ -78,6 +81,7 @@ ColDev col_dev(const amx_column* c)
     d.bits = c->bits;
     d.eps = c->format == AMX_SLAB ? 64 / c->bits : 0;
     d.magic = d.eps >= 2 ? (uint32_t)((1ull << 32) / d.eps + 1) : 0;
+    d.magic64 = magic64(d.eps);
     return d;
 }
 
@@ -101,6 +105,8 @@ OutDev out_dev(const amx_column* c)
     o.format = c->format;
     o.bits = c->bits;
     o.eps = c->format == AMX_SLAB ? 64 / c->bits : 0;
+    o.eps_m64 = magic64(o.eps);
+    o.bits_m64 = magic64(o.bits);
     return o;
 }
 

@@ -204,6 +204,10 @@ __device__ __forceinline__ uint64_t agg_decode(uint32_t agg, uint64_t a)
 
 __device__ __forceinline__ uint64_t mask_bits(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1); }
 
+// n / d for n < 2^58 and d in 1..64 with a precomputed magic m = floor(2^64 / d) + 1 (d >= 2):
+// a multiply-high instead of the long software 64-bit division
+__device__ __forceinline__ uint64_t udiv64(uint64_t n, uint64_t m, uint32_t d) { return d == 1 ? n : __umul64hi(n, m); }
+
 // ---------------------------------------------------------------------------------------------
 // runtime-width streaming reader over a staged copy of one column (shared memory)
 // ---------------------------------------------------------------------------------------------

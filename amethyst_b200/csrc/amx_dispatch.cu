@@ -26,7 +26,7 @@ static uint32_t stage_need(const ColDev& c, uint32_t tile_elems)
 template <class Pol>
 static amx_status launch(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
 {
-    constexpr uint32_t TILE = kPipeThreads * Pol::R;
+    constexpr uint32_t TILE = kPipeCompute * Pol::R;
     p.tile_elems = TILE;
     p.num_tiles = (p.n + TILE - 1) / TILE;
     const uint64_t need = sizeof(WsHeader) + 8 * p.num_tiles;
@@ -45,9 +45,19 @@ static amx_status launch(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t 
     if (p.has_mask_in) off += stage_need(p.m, TILE);
     p.stage_bytes = off;
     using V = typename Pol::V;
-    const uint32_t cv_entries = TILE + TILE / (sizeof(V) == 4 ? 32 : 16) + 1;  // bank skew padding
-    p.smem_fixed = p.has_out ? round_up(kCvOff + cv_entries * (uint32_t)sizeof(V), 128) : kCvOff;
-    const uint32_t smem = p.smem_fixed + kStages * p.stage_bytes;
+    p.smem_fixed = p.has_out ? round_up(kCvOff + TILE * (uint32_t)sizeof(V), 128) : kCvOff;
+    // Enough stages to keep ~64 KiB of each CTA's input in flight (HBM latency x bandwidth per
+    // SM slot), within the shared memory that lets Pol::kMinBlocks CTAs share an SM.
+    const uint32_t budget = Pol::kMinBlocks >= 2 ? 110 * 1024 : 220 * 1024;
+    // Compacting passes keep two stages: every held ticket delays the moment that tile's count
+    // is published, and the look-back of later tiles waits on it.
+    uint32_t stages = (64 * 1024 + p.stage_bytes - 1) / p.stage_bytes;
+    if (stages < 2) stages = 2;
+    if (stages > kMaxStages) stages = kMaxStages;
+    if (p.has_out && p.compact) stages = 2;
+    while (stages > 2 && p.smem_fixed + stages * p.stage_bytes > budget) stages--;
+    p.stages = stages;
+    const uint32_t smem = p.smem_fixed + stages * p.stage_bytes;
     if (smem > 227 * 1024) return fail(AMX_ERR_UNSUPPORTED, "pipeline needs %u bytes of shared memory", smem);
 
     cudaError_t e = cudaMemsetAsync(ws, 0, need, stream);
@@ -89,6 +99,29 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
     p.op = r.b ? r.op : AMX_OP_LHS;
     p.vbits = r.vbits;
     p.vmask = mask_of(r.vbits);
+    {
+        // op results that provably fit vbits need no masking
+        uint32_t widest = p.a.bits;
+        if (r.b) {
+            const uint32_t mx = p.a.bits > p.b.bits ? p.a.bits : p.b.bits;
+            switch (p.op) {
+                case AMX_OP_ADD: widest = mx + 1; break;
+                case AMX_OP_MUL: widest = p.a.bits + p.b.bits; break;
+                case AMX_OP_MIN:
+                case AMX_OP_MAX:
+                case AMX_OP_AND:
+                case AMX_OP_OR:
+                case AMX_OP_XOR: widest = mx; break;
+                case AMX_OP_DIV:
+                case AMX_OP_MOD:
+                case AMX_OP_LHS: widest = p.a.bits; break;
+                case AMX_OP_BOOL_OR:
+                case AMX_OP_BOOL_XOR: widest = 1; break;
+                default: widest = 64; break;  // sub wraps, math can be all ones
+            }
+        }
+        p.need_vmask = widest > r.vbits ? 1 : 0;
+    }
     if (r.pred) {
         amx_status st = normalize_pred(r.pred, p.pred_lo, p.pred_span, p.pred_neg);
         if (st) return st;

@@ -33,6 +33,7 @@ struct ChainReq {
 amx_status fail(amx_status s, const char* fmt, ...);
 amx_status cuda_fail(cudaError_t e, const char* what);
 uint64_t mask_of(uint32_t bits);
+uint64_t magic64(uint32_t d);
 uint64_t storage_bytes(uint32_t format, uint32_t bits, uint64_t n);
 amx_status check_column(const amx_column* c, const char* name);
 ColDev col_dev(const amx_column* c);

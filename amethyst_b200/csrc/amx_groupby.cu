@@ -1,0 +1,264 @@
+// amx_groupby.cu -- group-by sum + count over packed key and value columns.
+//
+// Replaces kernel_groupby_sm_array_gather / _writeout (src/kernels/groupby_sm_array.cuh:4-81) and
+// the sort-based CUB path (src/benchs/bench_groupby_sort_cub.cu:50-63).  Differences by design:
+// keys and values may have different formats and widths; sums are full uint64 (write them into a
+// narrower output column to get the reference's sums masked to the key width); counts are
+// emitted; groups come out in ascending key order (the reference's order is nondeterministic).
+//
+// 1. groupby_kernel: persistent CTAs of 512 threads walk chunks of 2^20 elements.  Lanes read
+//    consecutive elements (warp-major, coalesced) straight from the packed columns and aggregate
+//    into a per-CTA shared-memory table:
+//      - keys up to 12 bits: a dense table (sum as 32-bit low word + carry word, 32-bit count);
+//      - wider keys: an open-addressing hash table of 4096 slots (claimed by atomicCAS, linear
+//        probing, 8 probes); a key that finds no slot goes straight to the global table.
+//    Each chunk ends with a flush of the shared table into a dense global table of uint64 sums
+//    and counts (2^key_bits entries) with 64-bit atomics.
+// 2. the groups are extracted with the tile pipeline itself: mask = filter(count != 0), then
+//    compressstore of the key indices, the sums and the counts into the caller's output columns.
+#include "amx_dispatch.h"
+#include "amx_pipeline.cuh"
+
+namespace amx {
+
+constexpr uint32_t kGbThreads = 512;
+constexpr uint64_t kGbChunk = 1ull << 20;
+constexpr uint32_t kGbDenseBits = 12;
+constexpr uint32_t kGbHashSlots = 4096;
+constexpr uint32_t kGbMaxKeyBits = 24;
+constexpr uint32_t kEmptyKey = 0xffffffffu;
+
+struct GbParams {
+    ColDev k, v;
+    const uint32_t* mask;
+    uint64_t n;
+    uint32_t kbits;
+    uint32_t dense;
+    unsigned long long* gsum;
+    unsigned long long* gcnt;
+};
+
+// element e of column c read straight from global memory (consecutive lanes share words)
+__device__ __forceinline__ uint64_t load_elem(const ColDev& c, uint64_t e)
+{
+    switch (c.format) {
+        case AMX_PLAIN32: return __ldg(reinterpret_cast<const uint32_t*>(c.data) + e) & c.mask;
+        case AMX_PLAIN64: return __ldg(reinterpret_cast<const unsigned long long*>(c.data) + e) & c.mask;
+        case AMX_SLAB: {
+            const uint64_t s = udiv64(e, c.magic64, c.eps);
+            const uint32_t k = (uint32_t)(e - s * c.eps);
+            return (__ldg(reinterpret_cast<const unsigned long long*>(c.data) + s) >> (k * c.bits)) & c.mask;
+        }
+        default: {
+            const uint64_t bp = e * c.bits;
+            const uint64_t wi = bp >> 6;
+            const uint32_t off = (uint32_t)(bp & 63);
+            const unsigned long long* w = reinterpret_cast<const unsigned long long*>(c.data);
+            uint64_t x = __ldg(w + wi) >> off;
+            if (off + c.bits > 64) x |= (uint64_t)__ldg(w + wi + 1) << (64 - off);
+            return x & c.mask;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_constant__ GbParams p)
+{
+    extern __shared__ __align__(16) uint32_t tab[];
+    const uint32_t slots = p.dense ? (1u << p.kbits) : kGbHashSlots;
+    uint32_t* tkey = tab;                 // hash: key per slot
+    uint32_t* tlo = tab + slots;          // low 32 bits of the sum
+    uint32_t* thi = tab + 2 * slots;      // carries out of the low word
+    uint32_t* tcnt = tab + 3 * slots;     // count
+    const uint32_t tid = threadIdx.x;
+    const uint64_t nchunks = (p.n + kGbChunk - 1) / kGbChunk;
+
+    for (uint32_t i = tid; i < slots; i += blockDim.x) {
+        tkey[i] = kEmptyKey;
+        tlo[i] = thi[i] = tcnt[i] = 0;
+    }
+    __syncthreads();
+    for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const uint64_t e0 = chunk * kGbChunk;
+        const uint64_t e1 = e0 + kGbChunk < p.n ? e0 + kGbChunk : p.n;
+        for (uint64_t e = e0 + tid; e < e1; e += blockDim.x) {
+            if (p.mask && !((__ldg(p.mask + (e >> 5)) >> (e & 31)) & 1u)) continue;
+            const uint32_t key = (uint32_t)load_elem(p.k, e);
+            const uint32_t val = (uint32_t)load_elem(p.v, e);
+            uint32_t slot = key;
+            if (!p.dense) {
+                uint32_t h = (key * 2654435761u) >> 20;  // 12 bits: 4096 slots
+                slot = kEmptyKey;
+                for (int probe = 0; probe < 8; probe++) {
+                    const uint32_t sl = (h + probe) & (kGbHashSlots - 1);
+                    const uint32_t cur = tkey[sl];
+                    if (cur == key) {
+                        slot = sl;
+                        break;
+                    }
+                    if (cur == kEmptyKey) {
+                        const uint32_t prev = atomicCAS(&tkey[sl], kEmptyKey, key);
+                        if (prev == kEmptyKey || prev == key) {
+                            slot = sl;
+                            break;
+                        }
+                    }
+                }
+                if (slot == kEmptyKey) {  // table crowded: spill to the global table
+                    atomicAdd(&p.gsum[key], (unsigned long long)val);
+                    atomicAdd(&p.gcnt[key], 1ull);
+                    continue;
+                }
+            }
+            const uint32_t old = atomicAdd(&tlo[slot], val);
+            if (old + val < old) atomicAdd(&thi[slot], 1u);
+            atomicAdd(&tcnt[slot], 1u);
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < slots; i += blockDim.x) {
+            const uint32_t c = tcnt[i];
+            if (c) {
+                const uint32_t key = p.dense ? i : tkey[i];
+                atomicAdd(&p.gsum[key], ((unsigned long long)thi[i] << 32) | tlo[i]);
+                atomicAdd(&p.gcnt[key], (unsigned long long)c);
+            }
+            tkey[i] = kEmptyKey;
+            tlo[i] = thi[i] = tcnt[i] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+// Values wider than 32 bits: every element goes to the global table directly.
+__global__ void groupby_wide_kernel(const __grid_constant__ GbParams p)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < p.n; e += stride) {
+        if (p.mask && !((__ldg(p.mask + (e >> 5)) >> (e & 31)) & 1u)) continue;
+        const uint32_t key = (uint32_t)load_elem(p.k, e);
+        atomicAdd(&p.gsum[key], (unsigned long long)load_elem(p.v, e));
+        atomicAdd(&p.gcnt[key], 1ull);
+    }
+}
+
+__global__ void iota_kernel(uint32_t* out, uint64_t n)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)i;
+}
+
+static uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
+
+struct GbLayout {
+    uint64_t sums, counts, iota, mask, ws, total;
+};
+
+static GbLayout gb_layout(uint32_t kbits)
+{
+    const uint64_t g = 1ull << kbits;
+    GbLayout l;
+    l.sums = 0;
+    l.counts = align256(l.sums + 8 * g);
+    l.iota = align256(l.counts + 8 * g);
+    l.mask = align256(l.iota + 4 * g);
+    l.ws = align256(l.mask + 4 * ((g + 31) / 32) + 16);
+    l.total = align256(l.ws + amx_workspace_bytes(g));
+    return l;
+}
+
+}  // namespace amx
+
+using namespace amx;
+
+extern "C" {
+
+uint64_t amx_groupby_workspace_bytes(uint32_t key_bits)
+{
+    if (key_bits < 1 || key_bits > kGbMaxKeyBits) return 0;
+    return gb_layout(key_bits).total;
+}
+
+amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                       const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                       uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream)
+{
+    amx_status st = check_column(keys, "groupby: keys");
+    if (st) return st;
+    if ((st = check_column(vals, "groupby: values"))) return st;
+    if (keys->n != vals->n) return fail(AMX_ERR_INVALID_ARG, "groupby: keys and values lengths differ");
+    if (keys->bits > kGbMaxKeyBits)
+        return fail(AMX_ERR_UNSUPPORTED, "groupby: keys of %u bits (at most %u)", keys->bits, kGbMaxKeyBits);
+    if (((uintptr_t)d_mask) & 15) return fail(AMX_ERR_ALIGNMENT, "groupby: mask not 16-byte aligned");
+    const uint64_t g = 1ull << keys->bits;
+    const amx_column* outs[3] = {out_keys, out_sums, out_counts};
+    const char* names[3] = {"groupby: out_keys", "groupby: out_sums", "groupby: out_counts"};
+    for (int i = 0; i < 3; i++) {
+        if (!outs[i]) continue;
+        if ((st = check_column(outs[i], names[i]))) return st;
+        if (outs[i]->n < g) return fail(AMX_ERR_INVALID_ARG, "%s: capacity below 2^key_bits", names[i]);
+    }
+    const GbLayout L = gb_layout(keys->bits);
+    if (!ws || ws_bytes < L.total)
+        return fail(AMX_ERR_WORKSPACE, "groupby: workspace of %zu bytes, %llu needed", ws_bytes,
+                    (unsigned long long)L.total);
+    if (((uintptr_t)ws) & 255) return fail(AMX_ERR_ALIGNMENT, "groupby: workspace not 256-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    cudaError_t e = cudaMemsetAsync(w, 0, L.iota, s);  // sums and counts
+    if (e != cudaSuccess) return cuda_fail(e, "groupby: table clear");
+
+    GbParams p{};
+    p.k = col_dev(keys);
+    p.v = col_dev(vals);
+    p.mask = d_mask;
+    p.n = keys->n;
+    p.kbits = keys->bits;
+    p.dense = keys->bits <= kGbDenseBits;
+    p.gsum = reinterpret_cast<unsigned long long*>(w + L.sums);
+    p.gcnt = reinterpret_cast<unsigned long long*>(w + L.counts);
+    if (p.n) {
+        if (vals->bits <= 32) {
+            const uint32_t slots = p.dense ? (1u << p.kbits) : kGbHashSlots;
+            const size_t smem = 16ull * slots;
+            e = cudaFuncSetAttribute(groupby_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return cuda_fail(e, "groupby: shared memory attribute");
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, groupby_kernel, kGbThreads, smem);
+            uint64_t grid = (uint64_t)(per_sm > 0 ? per_sm : 1) * sm_count();
+            const uint64_t chunks = (p.n + kGbChunk - 1) / kGbChunk;
+            if (grid > chunks) grid = chunks;
+            groupby_kernel<<<(unsigned)grid, kGbThreads, smem, s>>>(p);
+        }
+        else {
+            groupby_wide_kernel<<<sm_count() * 8, 256, 0, s>>>(p);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: aggregation launch");
+    }
+    // groups: keys with a nonzero count, ascending
+    iota_kernel<<<(unsigned)((g + 255) / 256 < 4096 ? (g + 255) / 256 : 4096), 256, 0, s>>>(
+        reinterpret_cast<uint32_t*>(w + L.iota), g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: iota launch");
+    amx_column counts{w + L.counts, g, AMX_PLAIN64, 64};
+    amx_column sums{w + L.sums, g, AMX_PLAIN64, 64};
+    amx_column iota{w + L.iota, g, AMX_PLAIN32, 32};
+    uint32_t* mask = reinterpret_cast<uint32_t*>(w + L.mask);
+    void* pws = w + L.ws;
+    const size_t pws_bytes = L.total - L.ws;
+    const amx_predicate nonzero{AMX_PRED_NE, 64, 0, 0};
+    if ((st = amx_filter(&counts, &nonzero, mask, pws, pws_bytes, stream))) return st;
+    const amx_column* srcs[3] = {&iota, &sums, &counts};
+    bool counted = false;
+    for (int i = 0; i < 3; i++) {
+        if (!outs[i]) continue;
+        if ((st = amx_compressstore(srcs[i], mask, outs[i], counted ? nullptr : d_groups, pws, pws_bytes, stream)))
+            return st;
+        counted = true;
+    }
+    if (!counted && d_groups) {  // no output column: count the groups only
+        amx_chain_desc d{AMX_OP_LHS, 64, nonzero, AMX_AGG_SUM, 0};
+        if ((st = amx_chain(&d, &counts, nullptr, nullptr, nullptr, d_groups, nullptr, pws, pws_bytes, stream)))
+            return st;
+    }
+    return AMX_OK;
+}
+
+}  // extern "C"

@@ -21,7 +21,8 @@ struct ColDev {
     uint32_t format;
     uint32_t bits;
     uint32_t eps;    // elements per slab (slab format), else 0
-    uint32_t magic;  // floor(2^32 / eps) + 1 for eps >= 2: x / eps == umulhi(x, magic) for x < 2^17
+    uint32_t magic;    // floor(2^32 / eps) + 1 for eps >= 2: x / eps == umulhi(x, magic) for x < 2^17
+    uint64_t magic64;  // floor(2^64 / eps) + 1 for eps >= 2: n / eps == umul64hi(n, magic64) for n < 2^58
 };
 
 // Output column as the kernels see it.
@@ -32,6 +33,8 @@ struct OutDev {
     uint32_t bits;
     uint32_t eps;
     uint32_t pad;
+    uint64_t eps_m64;   // 64-bit magic divisors (see ColDev::magic64) for eps and for bits
+    uint64_t bits_m64;
 };
 
 // Workspace header, followed by one uint64 look-back status word per tile.
@@ -47,8 +50,9 @@ struct WsHeader {
 static_assert(sizeof(WsHeader) == 64, "workspace header layout");
 
 constexpr uint32_t kFmtMask = 7;  // internal format tag of an input bitmask column
-constexpr uint32_t kPipeThreads = 256;
-constexpr uint32_t kStages = 2;
+constexpr uint32_t kPipeCompute = 256;  // compute threads (8 warps) per CTA
+constexpr uint32_t kPipeThreads = kPipeCompute + 64;  // + loader warp + look-back warp
+constexpr uint32_t kMaxStages = 8;  // depth of the shared-memory staging ring (runtime: PipeParams::stages)
 
 // Parameters of the tile pipeline kernel (passed by value as a __grid_constant__).
 struct PipeParams {
@@ -70,7 +74,7 @@ struct PipeParams {
     uint32_t pred_lo32;   // 32-bit form of the predicate for values < 2^32 (pred32_ok)
     uint32_t pred_span32;
     uint32_t pred32_ok;
-    uint32_t pad2;
+    uint32_t need_vmask;  // 0 when op results provably fit vbits (masking is a no-op)
     uint32_t agg;
     uint32_t has_agg;
     uint32_t* mask_out;
@@ -82,6 +86,7 @@ struct PipeParams {
     uint64_t num_tiles;
     uint32_t tile_elems;
     uint32_t stage_bytes;  // bytes of one pipeline stage (a | b | m buffers)
+    uint32_t stages;       // stages in the ring, 2..kMaxStages
     uint32_t a_off, b_off, m_off;  // offsets of the buffers inside a stage
     uint32_t smem_fixed;           // bytes before the first stage
 };

@@ -1,18 +1,18 @@
 // amx_pipeline.cuh -- the tile pipeline kernel behind filter, compressstore, binary ops,
 // conversion, aggregation and fused chains.
 //
-// One persistent CTA per SM slot pulls tiles from an atomic ticket counter.  For each tile:
-//   1. one thread stages the tile's bytes of every input into shared memory with 1-D bulk
-//      copies (cp.async.bulk, completion on an mbarrier), two tiles ahead;
-//   2. every thread decodes R elements straight from the staged packed words (a policy:
-//      warp-major runtime-width readers, or thread-contiguous compile-time-width readers),
-//      applies the binary op and the predicate, and keeps a flag word;
-//   3. flags feed (a) the bitmask (warp ballots or a shared-memory bitmap), (b) the aggregate,
-//      (c) a block scan that publishes the tile's survivor count for the decoupled look-back
-//      and gathers the survivors into shared memory.
-//   4. the PREVIOUS tile's look-back (now short: its predecessors have had a whole tile of
-//      time to publish) gives its output offset, and its gathered survivors are re-encoded in
-//      the output format; boundary words shared with neighbouring tiles merge by atomics.
+// Persistent CTAs (two per SM) of ten warps with three roles, handing work over through
+// shared-memory mbarriers so that no compute warp ever waits on global-memory latency:
+//   * the loader warp (one lane) takes tiles from an atomic ticket counter and stages each
+//     tile's bytes of every input into a two-deep ring of shared-memory stages with 1-D bulk
+//     copies (cp.async.bulk, completion on the stage's `full` mbarrier);
+//   * eight compute warps decode R elements per thread straight from the staged packed words
+//     (a policy: warp-major runtime-width readers or thread-contiguous compile-time-width
+//     readers), apply the op and the predicate, build the bitmask / aggregate / count, scan the
+//     tile's survivors, publish the count for the decoupled look-back, gather the survivors in
+//     shared memory, and re-encode the PREVIOUS tile's survivors in the output format;
+//   * the look-back warp turns each tile's published count into its output offset (the tile's
+//     predecessors have had a whole tile of time to publish) and hands it to the compute warps.
 // Replaces the reference's separate filter / popcount / CUB scan / write kernels
 // (src/kernels/filter_slabs.cuh:4-57, src/kernels/compressstore_slabs.cuh:4-206,
 // src/benchs/bench_compressstore_slabs.cu:38-56) with one pass and no mask round trip.
@@ -28,7 +28,10 @@ __device__ __forceinline__ void col_range(const ColDev& c, uint64_t e0, uint64_t
     switch (c.format) {
         case AMX_PLAIN32: b0 = 4 * e0; b1 = 4 * e1; break;
         case AMX_PLAIN64: b0 = 8 * e0; b1 = 8 * e1; break;
-        case AMX_SLAB: b0 = 8 * (e0 / c.eps); b1 = 8 * ((e1 + c.eps - 1) / c.eps); break;
+        case AMX_SLAB:
+            b0 = 8 * udiv64(e0, c.magic64, c.eps);
+            b1 = 8 * udiv64(e1 + c.eps - 1, c.magic64, c.eps);
+            break;
         case AMX_NOGAPS: b0 = 8 * ((e0 * c.bits) >> 6); b1 = 8 * ((e1 * c.bits + 63) >> 6); break;
         default: b0 = 4 * (e0 >> 5); b1 = 4 * ((e1 + 31) >> 5); break;  // bitmask words
     }
@@ -62,7 +65,7 @@ __device__ __forceinline__ void stage_plan(const ColDev& c, uint64_t e0, uint64_
     for (uint64_t x = tend > s16 ? tend : s16; x < b1; x++) dst[x - s16] = src[x];
 }
 
-// Issue the staging of one tile into stage buffer `st` (called by a single thread).
+// Issue the staging of one tile into stage buffer `st` (one thread).
 __device__ __forceinline__ void stage_issue(const PipeParams& p, uint8_t* st, uint64_t* sbase, uint64_t* bar,
                                             uint64_t tile, uint32_t tile_elems)
 {
@@ -101,34 +104,25 @@ __device__ __forceinline__ V warp_incl_scan(V x)
     return x;
 }
 
-// Bank-skewed index of the gathered-values buffer: one pad entry per 32 (4-byte values) or
-// per 16 (8-byte values), so that strided per-thread access patterns spread over banks.
+// Re-encode cnt gathered values cv[0..cnt) as output elements [g, g+cnt), using the compute
+// threads (tid < nthreads).  Words wholly owned by this tile are stored; words shared with
+// neighbouring tiles are merged with atomicAnd (clear own bits) + atomicOr (set own bits), which
+// commute across tiles because owners are disjoint.  Dead slab bits belong to the owner of the
+// slab's last field; bits past the column's last element are cleared by the last tile (`last`).
 template <typename V>
-__device__ __forceinline__ uint32_t sk(uint32_t p)
+__device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32_t cnt, uint64_t g, bool last,
+                                            uint32_t tid, uint32_t T)
 {
-    return sizeof(V) == 4 ? p + (p >> 5) : p + (p >> 4);
-}
-
-// Re-encode cnt gathered values cv[0..cnt) as output elements [g, g+cnt).  Words wholly
-// owned by this tile are stored; words shared with neighbouring tiles are merged with
-// atomicAnd (clear own bits) + atomicOr (set own bits), which commute across tiles because
-// owners are disjoint.  Dead slab bits belong to the owner of the slab's last field; the
-// bits past the column's last element are cleared by the last tile (`last`).
-template <typename V>
-__device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32_t cnt, uint64_t g, bool last)
-{
-    const uint32_t tid = threadIdx.x;
-    const uint32_t T = blockDim.x;
     const uint64_t m = o.mask;
     switch (o.format) {
         case AMX_PLAIN32: {
             uint32_t* out = reinterpret_cast<uint32_t*>(o.data) + g;
-            for (uint32_t r = tid; r < cnt; r += T) out[r] = (uint32_t)((uint64_t)cv[sk<V>(r)] & m);
+            for (uint32_t r = tid; r < cnt; r += T) out[r] = (uint32_t)((uint64_t)cv[r] & m);
             return;
         }
         case AMX_PLAIN64: {
             uint64_t* out = reinterpret_cast<uint64_t*>(o.data) + g;
-            for (uint32_t r = tid; r < cnt; r += T) out[r] = (uint64_t)cv[sk<V>(r)] & m;
+            for (uint32_t r = tid; r < cnt; r += T) out[r] = (uint64_t)cv[r] & m;
             return;
         }
         case AMX_SLAB: {
@@ -136,12 +130,13 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
             const uint32_t eps = o.eps, b = o.bits;
             const uint64_t live = eps * b >= 64 ? ~0ull : ((1ull << (eps * b)) - 1);
             if (cnt) {
-                const uint64_t w0 = g / eps, w1 = (g + cnt - 1) / eps;
+                const uint64_t w0 = udiv64(g, o.eps_m64, eps), w1 = udiv64(g + cnt - 1, o.eps_m64, eps);
                 for (uint64_t w = w0 + tid; w <= w1; w += T) {
                     const int64_t r0 = (int64_t)(w * eps) - (int64_t)g;
                     uint64_t acc = 0;
                     if (r0 >= 0 && r0 + eps <= cnt) {
-                        for (uint32_t k = 0; k < eps; k++) acc |= ((uint64_t)cv[sk<V>((uint32_t)r0 + k)] & m) << (k * b);
+                        const V* c = cv + r0;
+                        for (uint32_t k = 0; k < eps; k++) acc |= ((uint64_t)c[k] & m) << (k * b);
                         out[w] = acc;
                     }
                     else {
@@ -149,7 +144,7 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
                         for (uint32_t k = 0; k < eps; k++) {
                             const int64_t r = r0 + k;
                             if (r >= 0 && r < (int64_t)cnt) {
-                                acc |= ((uint64_t)cv[sk<V>((uint32_t)r)] & m) << (k * b);
+                                acc |= ((uint64_t)cv[r] & m) << (k * b);
                                 own |= m << (k * b);
                             }
                         }
@@ -161,8 +156,9 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
             }
             if (last && tid == 0) {
                 const uint64_t total = g + cnt;
-                const uint32_t k = (uint32_t)(total % eps);
-                if (k) atomicAnd(&out[total / eps], (1ull << (k * b)) - 1);
+                const uint64_t tw = udiv64(total, o.eps_m64, eps);
+                const uint32_t k = (uint32_t)(total - tw * eps);
+                if (k) atomicAnd(&out[tw], (1ull << (k * b)) - 1);
             }
             return;
         }
@@ -176,13 +172,13 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
                     const uint64_t lo = w << 6, hi = lo + 64;
                     const uint64_t ob0 = lo > bit0 ? lo : bit0, ob1 = hi < bit1 ? hi : bit1;
                     const uint64_t own = (ob1 - ob0 >= 64) ? ~0ull : (((1ull << (ob1 - ob0)) - 1) << (ob0 - lo));
-                    uint64_t p0 = lo / b;
+                    uint64_t p0 = udiv64(lo, o.bits_m64, b);
                     if (p0 < g) p0 = g;
-                    uint64_t p1 = (hi - 1) / b;
+                    uint64_t p1 = udiv64(hi - 1, o.bits_m64, b);
                     if (p1 > g + cnt - 1) p1 = g + cnt - 1;
                     uint64_t acc = 0;
                     for (uint64_t q = p0; q <= p1; q++) {
-                        const uint64_t v = (uint64_t)cv[sk<V>((uint32_t)(q - g))] & m;
+                        const uint64_t v = (uint64_t)cv[q - g] & m;
                         const int64_t s = (int64_t)(q * b) - (int64_t)lo;
                         acc |= s >= 0 ? (v << s) : (v >> (-s));
                     }
@@ -205,9 +201,9 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
 
 // Look-back for a tile whose survivor count (AGG) is already published: returns the number
 // of survivors in all earlier tiles and publishes the tile's inclusive prefix (INC).  All 32
-// lanes of one warp call it.  Each round reads kLookWindow predecessor status words at once
-// (8 per lane, independent loads), so one round usually reaches a published prefix.  Every
-// wait is bounded: on timeout the error word is set and the missing value is taken as 0.
+// lanes of one warp call it.  Each round reads 256 predecessor status words at once (8 per
+// lane, independent loads), so one round usually reaches a published prefix.  Every wait is
+// bounded: on timeout the error word is set and the missing value is taken as 0.
 constexpr int kLookPerLane = 8;
 
 __device__ __forceinline__ uint64_t lookback_prev(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t* err)
@@ -216,19 +212,22 @@ __device__ __forceinline__ uint64_t lookback_prev(uint64_t* status, uint64_t til
     if (tile == 0) return 0;  // tile 0 published its inclusive prefix directly
     uint64_t excl = 0;
     int64_t j = (int64_t)tile - 1;
-    while (true) {
+    bool done = false;
+    while (!done) {
         uint64_t st[kLookPerLane];
 #pragma unroll
-        for (int m = 0; m < kLookPerLane; m++) {
+        for (int m = 0; m < kLookPerLane; m++) {  // all loads of the round in flight together
             const int64_t idx = j - (int64_t)(lane + 32 * m);
             st[m] = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
         }
-        // wait for unpublished predecessors (they are decoding now)
+        // consume the window nearest-first, 32 predecessors at a time, and stop at the first
+        // group holding an inclusive prefix: never wait on tiles beyond it
 #pragma unroll
         for (int m = 0; m < kLookPerLane; m++) {
+            if (done) break;
             const int64_t idx = j - (int64_t)(lane + 32 * m);
             uint32_t spins = 0;
-            while ((st[m] >> 62) == 0) {
+            while ((st[m] >> 62) == 0) {  // an earlier tile still decoding
                 if (++spins > kWaitSpins) {
                     record_error(err, AMX_ERR_TIMEOUT);
                     st[m] = kFlagInc;
@@ -237,56 +236,71 @@ __device__ __forceinline__ uint64_t lookback_prev(uint64_t* status, uint64_t til
                 if (spins > 8) __nanosleep(20);
                 st[m] = ld_relaxed_u64(&status[idx]);
             }
+            const uint32_t inc = __ballot_sync(0xffffffffu, (st[m] >> 62) == 2);
+            const int first = __ffs(inc) - 1;
+            uint64_t v = (first < 0 || (int)lane <= first) ? (st[m] & kValMask) : 0;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            excl += v;
+            done = first >= 0;
         }
-        // nearest inclusive prefix: smallest window position p = lane + 32 m
-        int mine = 1 << 30;
-#pragma unroll
-        for (int m = kLookPerLane - 1; m >= 0; m--)
-            if ((st[m] >> 62) == 2) mine = (int)lane + 32 * m;
-        int pmin = mine;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) pmin = min(pmin, __shfl_xor_sync(0xffffffffu, pmin, o));
-        uint64_t v = 0;
-#pragma unroll
-        for (int m = 0; m < kLookPerLane; m++)
-            if ((int)lane + 32 * m <= pmin) v += st[m] & kValMask;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        excl += v;
-        if (pmin < (1 << 30)) break;
         j -= 32 * kLookPerLane;
     }
     if (lane == 0) st_relaxed_u64(&status[tile], kFlagInc | (excl + agg));
     return excl;
 }
 
-// Shared-memory map of the pipeline kernel (dynamic shared memory):
-//   [0,64)     mbarriers            [64,128)  tickets        [128,256) stage base offsets
-//   [256,320)  warp totals          [320,384) broadcast      [384,448) warp aggregates
-//   [512,2560) tile bitmap (thread-contiguous policies, <= 16384 elements)
-//   [kCvOff, smem_fixed)  gathered values (bank-skewed);  [smem_fixed, ...) 2 stage buffers
-constexpr uint32_t kBitmapOff = 512;
-constexpr uint32_t kCvOff = 2560;
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void compute_bar()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(kPipeCompute) : "memory");
+}
+
+__device__ __forceinline__ void wait_or_flag(uint64_t* bar, uint32_t parity, uint32_t* err)
+{
+    if (!mbar_wait_bounded(bar, parity)) record_error(err, AMX_ERR_TIMEOUT);
+}
+
+// Shared-memory map (dynamic shared memory), for up to kMaxStages stages:
+//   [0,64) full[8]  [64,128) empty[8]  [128,144) agg[2]  [144,160) gready[2]   (mbarriers)
+//   [160,224)  tickets[8]              [224,416) stage base offsets [8][3]
+//   [416,480)  warp totals [2][8]      [480,544) warp counts      [544,592) per-slot tile / total / offset
+//   [608,672)  warp aggregates         [1024,3072) tile bitmap (thread-contiguous policies)
+//   [kCvOff, smem_fixed)  gathered values;  [smem_fixed, ...) p.stages stage buffers
+constexpr uint32_t kBitmapOff = 1024;
+constexpr uint32_t kCvOff = 3072;
+constexpr uint64_t kNoTile = ~0ull;
 
 template <class Pol>
-__global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constant__ PipeParams p)
+__global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(const __grid_constant__ PipeParams p)
 {
     using V = typename Pol::V;
     constexpr int R = Pol::R;
     constexpr bool WM = Pol::kWarpMajor;
-    constexpr uint32_t T = kPipeThreads;
+    constexpr uint32_t T = kPipeCompute;
     constexpr uint32_t NW = T / 32;
     constexpr uint32_t TILE = T * R;
     static_assert(TILE / 32 * 4 <= kCvOff - kBitmapOff, "bitmap region");
     static_assert(!WM || R <= 32, "warp-major runs keep one ballot per lane");
 
     extern __shared__ __align__(128) uint8_t smem[];
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem);
-    volatile uint64_t* tickets = reinterpret_cast<volatile uint64_t*>(smem + 64);
-    uint64_t* sbase = reinterpret_cast<uint64_t*>(smem + 128);
-    volatile uint64_t* warp_tot = reinterpret_cast<volatile uint64_t*>(smem + 256);
-    volatile uint64_t* bcast = reinterpret_cast<volatile uint64_t*>(smem + 320);
-    uint64_t* warp_agg = reinterpret_cast<uint64_t*>(smem + 384);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + kMaxStages;
+    uint64_t* aggb = full + 2 * kMaxStages;
+    uint64_t* gready = aggb + 2;
+    volatile uint64_t* tickets = reinterpret_cast<volatile uint64_t*>(smem + 160);
+    uint64_t* sbase = reinterpret_cast<uint64_t*>(smem + 224);
+    volatile uint32_t* warp_tot = reinterpret_cast<volatile uint32_t*>(smem + 416);
+    uint64_t* warp_cnt = reinterpret_cast<uint64_t*>(smem + 480);
+    volatile uint64_t* slot_tile = reinterpret_cast<volatile uint64_t*>(smem + 544);
+    volatile uint32_t* slot_total = reinterpret_cast<volatile uint32_t*>(smem + 560);
+    volatile uint64_t* slot_g = reinterpret_cast<volatile uint64_t*>(smem + 576);
+    uint64_t* warp_agg = reinterpret_cast<uint64_t*>(smem + 608);
+    const uint32_t S = p.stages;
     uint32_t* bitmap = reinterpret_cast<uint32_t*>(smem + kBitmapOff);
     V* cv = reinterpret_cast<V*>(smem + kCvOff);
     uint8_t* stage0 = smem + p.smem_fixed;
@@ -294,51 +308,108 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     if (tid == 0) {
-        for (uint32_t s = 0; s < kStages; s++) mbar_init(&mbar[s], 1);
+        for (uint32_t s = 0; s < S; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NW);
+        }
+        for (int q = 0; q < 2; q++) {
+            mbar_init(&aggb[q], 1);
+            mbar_init(&gready[q], 1);
+        }
         fence_mbar_init();
     }
     if (!WM)
-        for (uint32_t i = tid; i < TILE / 32; i += T) bitmap[i] = 0;
-    __syncthreads();
-    uint64_t next_tk = 0;  // thread 0: the ticket for the stage freed next
-    if (tid == 0) {
-        for (uint32_t s = 0; s < kStages; s++) {
-            const uint64_t tk = atomicAdd(&p.ws->ticket, 1u);
-            tickets[s] = tk;
-            if (tk < p.num_tiles) stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &mbar[s], tk, TILE);
-        }
-        next_tk = atomicAdd(&p.ws->ticket, 1u);
-    }
-    __syncthreads();
+        for (uint32_t i = tid; i < TILE / 32; i += blockDim.x) bitmap[i] = 0;
+    __syncthreads();  // the last CTA-wide barrier: roles split below
 
+    // ---------------------------------------------------------------- loader warp
+    if (warp == NW) {
+        if (lane == 0) {
+            // iteration j of the compute warps consumes stage j % S.  `stop_at` is the first
+            // iteration whose stage holds an invalid ticket: the compute warps leave the loop
+            // there, so they release no stage from that iteration on.
+            uint64_t stop_at = kNoTile;
+            for (uint32_t s = 0; s < S; s++) {
+                const uint64_t tk = stop_at == kNoTile ? atomicAdd(&p.ws->ticket, 1u) : p.num_tiles;
+                tickets[s] = tk;
+                if (tk < p.num_tiles)
+                    stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &full[s], tk, TILE);
+                else {
+                    mbar_arrive(&full[s]);
+                    if (stop_at == kNoTile) stop_at = s;
+                }
+            }
+            // the next ticket is taken one refill ahead, so its atomic latency overlaps the wait
+            uint64_t next = stop_at == kNoTile ? atomicAdd(&p.ws->ticket, 1u) : p.num_tiles;
+            uint32_t s = 0, phase = 0;
+            for (uint64_t j = 0; j < stop_at; j++) {
+                wait_or_flag(&empty[s], phase, &p.ws->err);  // iteration j released stage s
+                const uint64_t tk = stop_at == kNoTile ? next : p.num_tiles;
+                if (tk < p.num_tiles) next = atomicAdd(&p.ws->ticket, 1u);
+                tickets[s] = tk;  // for iteration j + S
+                if (tk < p.num_tiles)
+                    stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &full[s], tk, TILE);
+                else {
+                    mbar_arrive(&full[s]);
+                    if (stop_at == kNoTile) stop_at = j + S;
+                }
+                if (++s == S) {
+                    s = 0;
+                    phase ^= 1;
+                }
+            }
+        }
+        return;
+    }
+    // ---------------------------------------------------------------- look-back warp
+    if (warp == NW + 1) {
+        if (p.has_out && p.compact) {
+            for (uint32_t j = 0;; j++) {
+                const uint32_t q = j & 1;
+                wait_or_flag(&aggb[q], (j >> 1) & 1, &p.ws->err);
+                const uint64_t tile = slot_tile[q];
+                if (tile == kNoTile) break;
+                const uint64_t g = lookback_prev(p.status, tile, slot_total[q], &p.ws->err);
+                if (lane == 0) {
+                    slot_g[q] = g;
+                    mbar_arrive(&gready[q]);
+                }
+                __syncwarp();
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- compute warps
     uint64_t my_count = 0, my_agg = 0;
     bool have_prev = false;
     uint64_t prev_tile = 0;
-    uint32_t prev_total = 0;
+    uint32_t prev_total = 0, prev_j = 0;
 
-    // look-back (compacting) + encode of the previous tile's gathered survivors
     auto finish_prev = [&]() {
         uint64_t g;
         if (p.compact) {
-            if (warp == 0) {
-                const uint64_t x = lookback_prev(p.status, prev_tile, prev_total, &p.ws->err);
-                if (lane == 0) bcast[0] = x;
-            }
-            __syncthreads();
-            g = bcast[0];
+            wait_or_flag(&gready[prev_j & 1], (prev_j >> 1) & 1, &p.ws->err);
+            g = slot_g[prev_j & 1];
         }
         else {
             g = prev_tile * TILE;
         }
-        encode_tile<V>(p.out, cv, prev_total, g, prev_tile == p.num_tiles - 1);
-        __syncthreads();
+        encode_tile<V>(p.out, cv, prev_total, g, prev_tile == p.num_tiles - 1, tid, T);
+        compute_bar();  // cv is free
     };
 
-    for (uint32_t it = 0;; it++) {
-        const uint32_t s = it % kStages;
+    uint32_t j = 0, s = 0, sphase = 0;
+    for (;; j++) {
+        if (j) {
+            if (++s == S) {
+                s = 0;
+                sphase ^= 1;
+            }
+        }
+        wait_or_flag(&full[s], sphase, &p.ws->err);
         const uint64_t tile = tickets[s];
         if (tile >= p.num_tiles) break;
-        if (!mbar_wait_bounded(&mbar[s], (it / kStages) & 1)) record_error(&p.ws->err, AMX_ERR_TIMEOUT);
 
         const uint64_t e0 = tile * TILE;
         const uint64_t rem = p.n - e0;
@@ -361,6 +432,9 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
                 fl &= bits_at<R>(mw, tid * R);
             }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
+
         if (WM) {
             const uint32_t base = warp * 32 * R + lane;
             if (base + 32 * (R - 1) >= valid) {
@@ -378,18 +452,38 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
         }
         if (R < 64) fl &= (1ull << R) - 1;
 
-        __syncthreads();  // every thread is done with stage s
-        if (tid == 0) {
-            tickets[s] = next_tk;
-            if (next_tk < p.num_tiles)
-                stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &mbar[s], next_tk, TILE);
-            next_tk = atomicAdd(&p.ws->ticket, 1u);
-        }
-
         if (p.has_agg) {
+            uint64_t a = 0;
+            switch (p.agg) {
+                case AMX_AGG_SUM:
 #pragma unroll
-            for (int i = 0; i < R; i++)
-                if ((fl >> i) & 1) my_agg = agg_combine(p.agg, my_agg, agg_encode(p.agg, (uint64_t)v[i]));
+                    for (int i = 0; i < R; i++) a += ((fl >> i) & 1) ? (uint64_t)v[i] : 0;
+                    break;
+                case AMX_AGG_MIN:
+                case AMX_AGG_AND:
+#pragma unroll
+                    for (int i = 0; i < R; i++) {
+                        const uint64_t e = ((fl >> i) & 1) ? ~(uint64_t)v[i] : 0;
+                        a = p.agg == AMX_AGG_MIN ? (a > e ? a : e) : (a | e);
+                    }
+                    break;
+                case AMX_AGG_MAX:
+#pragma unroll
+                    for (int i = 0; i < R; i++) {
+                        const uint64_t e = ((fl >> i) & 1) ? (uint64_t)v[i] : 0;
+                        a = a > e ? a : e;
+                    }
+                    break;
+                case AMX_AGG_OR:
+#pragma unroll
+                    for (int i = 0; i < R; i++) a |= ((fl >> i) & 1) ? (uint64_t)v[i] : 0;
+                    break;
+                default:
+#pragma unroll
+                    for (int i = 0; i < R; i++) a ^= ((fl >> i) & 1) ? (uint64_t)v[i] : 0;
+                    break;
+            }
+            my_agg = agg_combine(p.agg, my_agg, a);
         }
 
         // ballots (warp-major) give mask words and in-warp ranks directly
@@ -420,20 +514,18 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
                 if (sh + R > 64) atomicOr(&bitmap[wi + 2], (uint32_t)(fl >> (64 - sh)));
             }
         }
-        // warp-major: c is the warp's count (same in every lane); thread-contiguous: own count
         my_count += WM ? (lane == 0 ? c : 0) : c;
 
         if (p.has_out) {
             // block scan: survivors before this thread (or warp) inside the tile
-            uint32_t pos, total;
+            volatile uint32_t* wt = warp_tot + 8 * (j & 1);
+            uint32_t pos, total = 0, before = 0;
             if (WM) {
-                if (lane == 0) warp_tot[warp] = c;
-                __syncthreads();
-                uint32_t before = 0;
-                total = 0;
+                if (lane == 0) wt[warp] = c;
+                compute_bar();
 #pragma unroll
                 for (uint32_t w = 0; w < NW; w++) {
-                    const uint32_t x = (uint32_t)warp_tot[w];
+                    const uint32_t x = wt[w];
                     before += w < warp ? x : 0;
                     total += x;
                 }
@@ -441,48 +533,57 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
             }
             else {
                 const uint32_t incl = warp_incl_scan<uint32_t>(c);
-                if (lane == 31) warp_tot[warp] = incl;
-                __syncthreads();
-                uint32_t before = 0;
-                total = 0;
+                if (lane == 31) wt[warp] = incl;
+                compute_bar();
 #pragma unroll
                 for (uint32_t w = 0; w < NW; w++) {
-                    const uint32_t x = (uint32_t)warp_tot[w];
+                    const uint32_t x = wt[w];
                     before += w < warp ? x : 0;
                     total += x;
                 }
                 pos = before + incl - c;
             }
-            if (p.compact && tid == 0) st_relaxed_u64(&p.status[tile], (tile == 0 ? kFlagInc : kFlagAgg) | total);
+            if (p.compact && tid == 0) {
+                st_relaxed_u64(&p.status[tile], (tile == 0 ? kFlagInc : kFlagAgg) | total);
+                slot_tile[j & 1] = tile;
+                slot_total[j & 1] = total;
+                mbar_arrive(&aggb[j & 1]);  // hand the tile to the look-back warp
+            }
 
-            if (have_prev) finish_prev();  // ends with __syncthreads: cv is free
+            if (have_prev) finish_prev();  // ends with a compute barrier: cv is free
 
             if (WM) {
                 const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
                 for (int i = 0; i < R; i++) {
-                    if ((fl >> i) & 1) cv[sk<V>(pos + __popc(bal[i] & lt))] = v[i];
+                    if ((fl >> i) & 1) cv[pos + __popc(bal[i] & lt)] = v[i];
                     pos += __popc(bal[i]);
                 }
             }
             else {
+                V* dst = cv + pos;
 #pragma unroll
                 for (int i = 0; i < R; i++)
-                    if ((fl >> i) & 1) cv[sk<V>(pos++)] = v[i];
+                    if ((fl >> i) & 1) *dst++ = v[i];
             }
             have_prev = true;
             prev_tile = tile;
             prev_total = total;
+            prev_j = j;
         }
         if (!WM && p.mask_out) {
-            __syncthreads();
+            compute_bar();
             const uint32_t words = (valid + 31) / 32;
             for (uint32_t i = tid; i < words; i += T) {
                 p.mask_out[e0 / 32 + i] = bitmap[i];
                 bitmap[i] = 0;
             }
+            compute_bar();
         }
-        __syncthreads();
+    }
+    if (p.has_out && p.compact && tid == 0) {  // release the look-back warp
+        slot_tile[j & 1] = kNoTile;
+        mbar_arrive(&aggb[j & 1]);
     }
     if (have_prev) finish_prev();
 
@@ -492,16 +593,16 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
         my_count += __shfl_xor_sync(0xffffffffu, my_count, o);
         my_agg = agg_combine(p.agg, my_agg, __shfl_xor_sync(0xffffffffu, my_agg, o));
     }
-    __syncthreads();
+    compute_bar();
     if (lane == 0) {
-        warp_tot[warp] = my_count;
+        warp_cnt[warp] = my_count;
         warp_agg[warp] = my_agg;
     }
-    __syncthreads();
+    compute_bar();
     if (tid == 0) {
         uint64_t cnt = 0, ag = 0;
         for (uint32_t w = 0; w < NW; w++) {
-            cnt += warp_tot[w];
+            cnt += warp_cnt[w];
             ag = agg_combine(p.agg, ag, warp_agg[w]);
         }
         atomicAdd(&p.ws->count, (unsigned long long)cnt);
@@ -524,8 +625,10 @@ __global__ void __launch_bounds__(kPipeThreads) pipe_kernel(const __grid_constan
 template <int R_, typename V>
 __device__ __forceinline__ void finish_values(const PipeParams& p, V (&v)[R_], uint64_t& fl)
 {
+    if (p.need_vmask) {
 #pragma unroll
-    for (int i = 0; i < R_; i++) v[i] = (V)((uint64_t)v[i] & p.vmask);
+        for (int i = 0; i < R_; i++) v[i] = (V)((uint64_t)v[i] & p.vmask);
+    }
     if (p.has_pred) {
         const PredN pn{p.pred_lo, p.pred_span, p.pred_neg, 0};
         fl = 0;
@@ -561,7 +664,7 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
             break;
         }
         case AMX_SLAB: {
-            const uint64_t s0 = e0 / c.eps;
+            const uint64_t s0 = udiv64(e0, c.magic64, c.eps);
             const uint32_t r0 = (uint32_t)(e0 - s0 * c.eps);
             const uint64_t* w = reinterpret_cast<const uint64_t*>(st) + (s0 - sb / 8);
             const uint32_t eps = c.eps, b = c.bits, mg = c.magic;
@@ -595,6 +698,7 @@ struct GenericPol {
     using V = uint64_t;
     static constexpr int R = 16;
     static constexpr bool kWarpMajor = true;
+    static constexpr int kMinBlocks = 1;
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
                                                   uint64_t e0, V (&v)[R], uint64_t& fl)

@@ -3,8 +3,8 @@
 //
 // A policy fixes R (elements per thread per tile) and decodes a thread's run of R elements
 // from the staged words.  GenericPol (amx_pipeline.cuh) handles any format and width with
-// runtime streaming readers.  The policies here fix the slab widths at compile time so
-// every shift and mask is a constant and each thread's run starts on a slab boundary:
+// warp-major runtime readers.  The policies here fix the slab widths at compile time so every
+// shift and mask is a constant and each thread's run starts on a slab boundary:
 //   SlabPol<B>           one slab column of width B (filter, compressstore, reduce, convert)
 //   Slab2Pol<BA, BB>     two slab columns (binary op, fused chains)
 // Values are 32-bit, so these policies serve value widths up to 32.
@@ -61,7 +61,7 @@ __device__ __forceinline__ void unpack_slabs(const uint64_t (&w)[N], uint32_t (&
 template <int R>
 __device__ __forceinline__ void finish32(const PipeParams& p, uint32_t (&v)[R], uint64_t& fl)
 {
-    if (p.vbits < 32) {
+    if (p.need_vmask) {
         const uint32_t vm = (uint32_t)p.vmask;
 #pragma unroll
         for (int i = 0; i < R; i++) v[i] &= vm;
@@ -73,8 +73,14 @@ __device__ __forceinline__ void finish32(const PipeParams& p, uint32_t (&v)[R], 
     fl = 0;
     if (p.pred32_ok) {
         const uint32_t lo = p.pred_lo32, span = p.pred_span32;
+        if (lo == 0) {
 #pragma unroll
-        for (int i = 0; i < R; i++) fl |= (uint64_t)((v[i] - lo) <= span) << i;
+            for (int i = 0; i < R; i++) fl |= (uint64_t)(v[i] <= span) << i;
+        }
+        else {
+#pragma unroll
+            for (int i = 0; i < R; i++) fl |= (uint64_t)((v[i] - lo) <= span) << i;
+        }
         if (p.pred_neg) fl = ~fl;
     }
     else {
@@ -91,6 +97,7 @@ struct SlabPol {
     static constexpr int SPT = EPS >= 32 ? 1 : 32 / EPS;
     static constexpr int R = EPS * SPT;
     static constexpr bool kWarpMajor = false;
+    static constexpr int kMinBlocks = R > 40 ? 1 : 2;
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
                                                   uint64_t e0, V (&v)[R], uint64_t& fl)
@@ -104,27 +111,15 @@ struct SlabPol {
     }
 };
 
-template <int R>
-__device__ __forceinline__ void apply_op32(uint32_t op, uint32_t (&v)[R], const uint32_t (&r)[R])
+// v[j*EPS + k] = op(v[j*EPS + k], field k of slab j), in place (no second value array)
+template <int B, int EPS, int N, int R, typename F>
+__device__ __forceinline__ void combine_slabs(const uint64_t (&w)[N], uint32_t (&v)[R], F f)
 {
-    switch (op) {
-        case AMX_OP_ADD:
 #pragma unroll
-            for (int i = 0; i < R; i++) v[i] += r[i];
-            break;
-        case AMX_OP_SUB:
+    for (int j = 0; j < N; j++)
 #pragma unroll
-            for (int i = 0; i < R; i++) v[i] -= r[i];
-            break;
-        case AMX_OP_MUL:
-#pragma unroll
-            for (int i = 0; i < R; i++) v[i] *= r[i];
-            break;
-        default:
-#pragma unroll
-            for (int i = 0; i < R; i++) v[i] = (uint32_t)binop_eval(op, v[i], r[i]);
-            break;
-    }
+        for (int k = 0; k < EPS; k++)
+            v[j * EPS + k] = f(v[j * EPS + k], (uint32_t)((w[j] >> (k * B)) & ((1ull << B) - 1)));
 }
 
 template <int BA, int BB>
@@ -137,6 +132,7 @@ struct Slab2Pol {
     static constexpr int SA = R / EA;
     static constexpr int SB = R / EB;
     static constexpr bool kWarpMajor = false;
+    static constexpr int kMinBlocks = R > 40 ? 1 : 2;
     static_assert(R <= 64, "run too long for the flag word");
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
@@ -149,14 +145,21 @@ struct Slab2Pol {
             lds_words<SA>(w, s);
             unpack_slabs<BA, EA, SA, R>(s, v);
         }
-        uint32_t r[R];
         {
             const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.b_off) + (first / EB - sb[1] / 8);
             uint64_t s[SB];
             lds_words<SB>(w, s);
-            unpack_slabs<BB, EB, SB, R>(s, r);
+            switch (p.op) {
+                case AMX_OP_ADD: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a + b; }); break;
+                case AMX_OP_SUB: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a - b; }); break;
+                case AMX_OP_MUL: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a * b; }); break;
+                case AMX_OP_MIN: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a < b ? a : b; }); break;
+                case AMX_OP_MAX: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a > b ? a : b; }); break;
+                case AMX_OP_AND: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a & b; }); break;
+                case AMX_OP_OR: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a | b; }); break;
+                default: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a ^ b; }); break;
+            }
         }
-        apply_op32<R>(p.op, v, r);
         finish32<R>(p, v, fl);
     }
 };
@@ -184,7 +187,10 @@ inline int choose_policy(const PipeParams& p, int force)
     const bool a_slab = p.a.format == AMX_SLAB && p.a.bits <= 32;
     int auto_id = 0;
     if (v32 && a_slab && !p.has_b) auto_id = (int)p.a.bits;
-    if (v32 && a_slab && p.has_b && p.b.format == AMX_SLAB) {
+    // two-column compile-time policies cover the 32-bit-exact ops; the rest take the generic path
+    const bool cheap_op = p.op == AMX_OP_ADD || p.op == AMX_OP_SUB || p.op == AMX_OP_MUL || p.op == AMX_OP_MIN ||
+                          p.op == AMX_OP_MAX || p.op == AMX_OP_AND || p.op == AMX_OP_OR || p.op == AMX_OP_XOR;
+    if (v32 && a_slab && p.has_b && p.b.format == AMX_SLAB && cheap_op) {
 #define AMX_PAIR_MATCH(id, x, y) \
     if (p.a.bits == x && p.b.bits == y) auto_id = id;
         AMX_SLAB2_PAIRS(AMX_PAIR_MATCH)

@@ -154,5 +154,24 @@ def chain(lhs: PackedColumn, rhs: PackedColumn | None, op: int, value_bits: int,
     return out, mask, cnt, ag
 
 
+def groupby(keys: PackedColumn, vals: PackedColumn, key_fmt: int = A.PLAIN32, sum_fmt: int = A.PLAIN64,
+            sum_bits: int = 64, count_fmt: int | None = A.PLAIN64, mask: torch.Tensor | None = None, ws=None,
+            stream=None):
+    """Group-by sum + count (kernel_groupby_sm_array's successor): returns (keys, sums, counts,
+    groups tensor) with groups in ascending key order."""
+    dev = keys.data.device
+    g = 1 << keys.bits
+    ok = PackedColumn.empty(g, key_fmt, keys.bits if key_fmt != A.PLAIN32 or keys.bits <= 32 else 32, dev)
+    os_ = PackedColumn.empty(g, sum_fmt, sum_bits, dev)
+    oc = PackedColumn.empty(g, count_fmt, 64 if count_fmt != A.PLAIN32 else 32, dev) if count_fmt is not None else None
+    ng = torch.zeros(2, dtype=torch.int64, device=dev)
+    if ws is None:
+        ws = torch.empty(int(lib().amx_groupby_workspace_bytes(keys.bits)), dtype=torch.uint8, device=dev)
+    check(lib().amx_groupby(C.byref(keys.desc), C.byref(vals.desc), _ptr(mask), C.byref(ok.desc), C.byref(os_.desc),
+                            C.byref(oc.desc) if oc is not None else None, _ptr(ng), _ptr(ws), ws.numel(),
+                            _stream_ptr(stream)))
+    return ok, os_, oc, ng
+
+
 def workspace_status(ws: torch.Tensor, stream=None) -> None:
     check(lib().amx_workspace_status(_ptr(ws), _stream_ptr(stream)))

@@ -174,6 +174,20 @@ amx_status amx_convert(const amx_column* in, const amx_column* out, void* worksp
 amx_status amx_reduce(uint32_t agg, const amx_column* in, const uint32_t* d_mask, uint64_t* d_result,
                       void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- group-by ---------------------------------------------------------------------------- */
+/* Group-by sum + count: for every distinct key (ascending) the key, the uint64 sum of its values
+ * and its count, compressed into the three output columns (each may be NULL; capacity >=
+ * 2^key_bits); the number of groups goes to *d_groups.  Keys: any format, at most 24 bits.
+ * Values: any format and width.  Optional d_mask restricts the input to the masked elements.
+ * Writing sums into a narrower column masks them, which gives the reference's aggregate
+ * (sum masked to the key width).  Replaces kernel_groupby_sm_array_gather/_writeout
+ * (src/kernels/groupby_sm_array.cuh:4-81) and the sort-based path
+ * (src/benchs/bench_groupby_sort_cub.cu:50-63).  The workspace must be 256-byte aligned. */
+uint64_t amx_groupby_workspace_bytes(uint32_t key_bits);
+amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                       const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                       uint64_t* d_groups, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- fused operator chain -------------------------------------------------------------- */
 /* v = op(lhs, rhs) masked to value_bits (v = lhs when rhs is NULL), keep the elements with
  * pred(v), then any of: the survivors compacted into `out`, the bitmask of pred(v) into

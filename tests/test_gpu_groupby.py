@@ -1,0 +1,82 @@
+"""Group-by sum + count against the oracle's dense group table, bit-exact, through the C ABI."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import NOGAPS, PLAIN32, PLAIN64, SLAB, gpu_bytes, make_column, to_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def zipf_keys(n, groups, s, seed):
+    from amethyst_b200.datagen import zipf_cdf
+
+    cdf = zipf_cdf(groups, s)
+    u = np.random.default_rng(seed).random(n)
+    return np.searchsorted(cdf, u, side="right").astype(np.uint64)
+
+
+CASES = [
+    # key fmt, key bits, val fmt, val bits, n, key distribution
+    (SLAB, 10, SLAB, 16, 1 << 20, "zipf"),      # the group-by configuration at reduced size
+    (SLAB, 10, SLAB, 10, 300001, "zipf"),       # the reference's layout: keys and values share b
+    (PLAIN32, 12, PLAIN32, 32, 200003, "uniform"),
+    (NOGAPS, 7, NOGAPS, 13, 123457, "uniform"),
+    (SLAB, 16, SLAB, 16, 500000, "zipf"),       # hash path
+    (SLAB, 20, PLAIN32, 20, 400001, "uniform"),  # hash path with spills
+    (PLAIN64, 24, SLAB, 7, 100000, "uniform"),
+    (SLAB, 11, PLAIN64, 40, 77777, "zipf"),     # values wider than 32 bits
+    (SLAB, 3, SLAB, 5, 4096, "uniform"),
+    (SLAB, 5, SLAB, 5, 0, "uniform"),
+    (SLAB, 5, SLAB, 5, 1, "uniform"),
+]
+
+
+@pytest.mark.parametrize("kf,kb,vf,vb,n,dist", CASES)
+def test_groupby_matches_oracle(cuda, kf, kb, vf, vb, n, dist):
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    keys = zipf_keys(n, min(1000, 1 << kb), 1.1, kb * 7 + n) if dist == "zipf" else None
+    kv, kraw = make_column(kb * 101 + n, kf, kb, n, vals=keys)
+    vv, vraw = make_column(vb * 103 + n, vf, vb, n)
+    kc, vc = to_gpu(kraw, n, kf, kb), to_gpu(vraw, n, vf, vb)
+    groups, sums, counts = O.groupby_dense(kraw, kf, kb, vraw, vf, vb, n)
+    present = np.nonzero(counts)[0].astype(np.uint64)
+    for sum_fmt, sum_bits in [(PLAIN64, 64), (SLAB, kb)]:
+        ok, osum, ocnt, ng = ops.groupby(kc, vc, key_fmt=SLAB, sum_fmt=sum_fmt, sum_bits=sum_bits,
+                                         count_fmt=PLAIN64)
+        g = int(ng[0].item())
+        assert g == groups
+        assert np.array_equal(gpu_bytes(ok, g), O.encode(SLAB, kb, present)[: O.storage_bytes(SLAB, kb, g)])
+        assert np.array_equal(gpu_bytes(osum, g),
+                              O.encode(sum_fmt, sum_bits, sums[present.astype(np.int64)])[
+                                  : O.storage_bytes(sum_fmt, sum_bits, g)])
+        assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), counts[present.astype(np.int64)])
+
+
+def test_groupby_with_mask(cuda):
+    import torch
+
+    from amethyst_b200 import ops
+
+    n = 250001
+    keys = zipf_keys(n, 1000, 1.1, 3)
+    kv, kraw = make_column(1, SLAB, 10, n, vals=keys)
+    vv, vraw = make_column(2, SLAB, 16, n)
+    m = np.random.default_rng(4).integers(0, 2**32, size=(n + 31) // 32, dtype=np.uint64).astype(np.uint32)
+    m[-1] &= np.uint32((1 << (n % 32)) - 1)
+    dm = torch.zeros(len(m) + 4, dtype=torch.int32, device="cuda")
+    dm[: len(m)].copy_(torch.from_numpy(m.view(np.int32)))
+    sel = np.unpackbits(m.view(np.uint8), bitorder="little")[:n].astype(bool)
+    want_sum = np.zeros(1024, np.uint64)
+    want_cnt = np.zeros(1024, np.uint64)
+    np.add.at(want_sum, kv[sel].astype(np.int64), vv[sel])
+    np.add.at(want_cnt, kv[sel].astype(np.int64), 1)
+    ok, osum, ocnt, ng = ops.groupby(to_gpu(kraw, n, SLAB, 10), to_gpu(vraw, n, SLAB, 16), key_fmt=PLAIN32, mask=dm)
+    present = np.nonzero(want_cnt)[0]
+    g = int(ng[0].item())
+    assert g == len(present)
+    assert np.array_equal(gpu_bytes(ok, g).view(np.uint32), present.astype(np.uint32))
+    assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), want_sum[present])
+    assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), want_cnt[present])
