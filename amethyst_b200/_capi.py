@@ -39,6 +39,11 @@ class ChainDesc(C.Structure):
                 ("agg", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("staged_bytes", C.c_uint32), ("compact_stages", C.c_uint32), ("policy", C.c_int32),
+                ("reserved", C.c_uint32)]
+
+
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libamethyst_b200.so")
 
 _P = C.c_void_p
@@ -52,6 +57,8 @@ _SIGS = {
     "amx_binary_out_bits": (C.c_uint32, [C.c_uint32, C.c_uint32, C.c_uint32]),
     "amx_workspace_bytes": (C.c_uint64, [C.c_uint64]),
     "amx_workspace_status": (C.c_int, [_P, _P]),
+    "amx_set_tuning": (C.c_int, [C.POINTER(Tuning)]),
+    "amx_get_tuning": (C.c_int, [C.POINTER(Tuning)]),
     "amx_filter": (C.c_int, [_COL, C.POINTER(Predicate), _P, _P, C.c_size_t, _P]),
     "amx_compressstore": (C.c_int, [_COL, _P, _COL, _P, _P, C.c_size_t, _P]),
     "amx_filter_compressstore": (C.c_int, [_COL, C.POINTER(Predicate), _COL, _P, _P, C.c_size_t, _P]),

@@ -211,6 +211,19 @@ const char* amx_status_string(amx_status s)
 
 const char* amx_last_error(void) { return g_last_error.c_str(); }
 
+amx_status amx_set_tuning(const amx_tuning* t)
+{
+    tuning() = t ? *t : amx_tuning{};
+    return AMX_OK;
+}
+
+amx_status amx_get_tuning(amx_tuning* t)
+{
+    if (!t) return fail(AMX_ERR_INVALID_ARG, "get_tuning: null output");
+    *t = tuning();
+    return AMX_OK;
+}
+
 uint64_t amx_storage_bytes(uint32_t format, uint32_t bits, uint64_t n)
 {
     if (!width_ok(format, bits)) return 0;

@@ -85,49 +85,6 @@ __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p)
 
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t code) { atomicCAS(err, 0u, code); }
 
-// Decoupled look-back (single-pass chained scan).  Called by all 32 lanes of one warp with
-// the tile's survivor count; returns the number of survivors in all earlier tiles.  Every
-// wait is bounded: on timeout the error word is set and the missing prefix is taken as 0.
-__device__ __forceinline__ uint64_t lookback(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t* err)
-{
-    const uint32_t lane = threadIdx.x & 31;
-    if (tile == 0) {
-        if (lane == 0) st_relaxed_u64(&status[0], kFlagInc | agg);
-        return 0;
-    }
-    if (lane == 0) st_relaxed_u64(&status[tile], kFlagAgg | agg);
-    uint64_t excl = 0;
-    int64_t j = (int64_t)tile - 1;
-    while (true) {
-        const int64_t idx = j - (int64_t)lane;
-        uint64_t st = kFlagInc;  // before tile 0: an inclusive prefix of 0
-        if (idx >= 0) {
-            uint32_t spins = 0;
-            st = ld_relaxed_u64(&status[idx]);
-            while ((st >> 62) == 0) {
-                if (++spins > kWaitSpins) {
-                    record_error(err, AMX_ERR_TIMEOUT);
-                    st = kFlagInc;
-                    break;
-                }
-                if (spins > 32) __nanosleep(32);
-                st = ld_relaxed_u64(&status[idx]);
-            }
-        }
-        const uint32_t inc = __ballot_sync(0xffffffffu, (st >> 62) == 2);
-        const int first = __ffs(inc) - 1;
-        uint64_t v = st & kValMask;
-        if (first >= 0 && (int)lane > first) v = 0;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        excl += v;
-        if (first >= 0) break;
-        j -= 32;
-    }
-    if (lane == 0) st_relaxed_u64(&status[tile], kFlagInc | (excl + agg));
-    return excl;
-}
-
 // ---------------------------------------------------------------------------------------------
 // predicate and operator evaluation
 // ---------------------------------------------------------------------------------------------
@@ -207,83 +164,5 @@ __device__ __forceinline__ uint64_t mask_bits(uint32_t bits) { return bits >= 64
 // n / d for n < 2^58 and d in 1..64 with a precomputed magic m = floor(2^64 / d) + 1 (d >= 2):
 // a multiply-high instead of the long software 64-bit division
 __device__ __forceinline__ uint64_t udiv64(uint64_t n, uint64_t m, uint32_t d) { return d == 1 ? n : __umul64hi(n, m); }
-
-// ---------------------------------------------------------------------------------------------
-// runtime-width streaming reader over a staged copy of one column (shared memory)
-// ---------------------------------------------------------------------------------------------
-// `base` is the staged bytes; `first` is the column element the stream starts at and `sbyte`
-// the column byte offset the stage starts at.
-struct Stream {
-    const uint8_t* base;
-    uint64_t cur;   // slab: remaining fields; nogaps: low word of the window
-    uint64_t nxt;   // nogaps: high word of the window
-    uint32_t word;  // index of the current 8-byte word (slab/nogaps) or element (plain)
-    uint32_t left;  // slab: fields left in cur; nogaps: bit offset in the window
-    uint32_t fmt, bits, eps;
-    uint64_t m;
-
-    __device__ __forceinline__ void init(const ColDev& c, const uint8_t* stage, uint64_t sbyte, uint64_t first)
-    {
-        base = stage;
-        fmt = c.format;
-        bits = c.bits;
-        eps = c.eps;
-        m = c.mask;
-        const uint64_t* w = reinterpret_cast<const uint64_t*>(stage);
-        switch (fmt) {
-            case AMX_PLAIN32: word = (uint32_t)(first - sbyte / 4); break;
-            case AMX_PLAIN64: word = (uint32_t)(first - sbyte / 8); break;
-            case AMX_SLAB: {
-                const uint64_t s = first / eps;
-                const uint32_t k = (uint32_t)(first - s * eps);
-                word = (uint32_t)(s - sbyte / 8);
-                cur = k ? (w[word] >> (k * bits)) : w[word];
-                left = eps - k;
-                break;
-            }
-            default: {  // nogaps
-                const uint64_t bitpos = first * bits - sbyte * 8;
-                word = (uint32_t)(bitpos >> 6);
-                left = (uint32_t)(bitpos & 63);
-                cur = w[word];
-                nxt = w[word + 1];
-                break;
-            }
-        }
-    }
-
-    __device__ __forceinline__ uint64_t next()
-    {
-        const uint64_t* w = reinterpret_cast<const uint64_t*>(base);
-        uint64_t v;
-        switch (fmt) {
-            case AMX_PLAIN32: v = reinterpret_cast<const uint32_t*>(base)[word++]; break;
-            case AMX_PLAIN64: v = w[word++]; break;
-            case AMX_SLAB:
-                v = cur;
-                cur = bits < 64 ? (cur >> bits) : 0;
-                if (--left == 0) {
-                    cur = w[++word];
-                    left = eps;
-                }
-                break;
-            default: {
-                const uint32_t off = left;
-                v = off ? ((cur >> off) | (nxt << (64 - off))) : cur;
-                const uint32_t e = off + bits;
-                if (e >= 64) {
-                    cur = nxt;
-                    nxt = w[++word + 1];
-                    left = e - 64;
-                }
-                else {
-                    left = e;
-                }
-                break;
-            }
-        }
-        return v & m;
-    }
-};
 
 }  // namespace amx

@@ -30,6 +30,9 @@ struct ChainReq {
     int force_policy = -1;  // -1 = automatic; otherwise a policy id (tests and the autotuner)
 };
 
+// launch tuning of this host thread (amx_set_tuning); zero fields mean "automatic"
+amx_tuning& tuning();
+
 amx_status fail(amx_status s, const char* fmt, ...);
 amx_status cuda_fail(cudaError_t e, const char* what);
 uint64_t mask_of(uint32_t bits);

@@ -50,9 +50,8 @@ struct WsHeader {
 static_assert(sizeof(WsHeader) == 64, "workspace header layout");
 
 constexpr uint32_t kFmtMask = 7;  // internal format tag of an input bitmask column
-constexpr uint32_t kPipeCompute = 256;  // compute threads (8 warps) per CTA
-constexpr uint32_t kPipeThreads = kPipeCompute + 64;  // + loader warp + look-back warp
 constexpr uint32_t kMaxStages = 8;  // depth of the shared-memory staging ring (runtime: PipeParams::stages)
+constexpr uint32_t kMaxSlots = 4;   // gathered-value slots of a compacting pass (runtime: PipeParams::slots)
 
 // Parameters of the tile pipeline kernel (passed by value as a __grid_constant__).
 struct PipeParams {
@@ -87,7 +86,13 @@ struct PipeParams {
     uint32_t tile_elems;
     uint32_t stage_bytes;  // bytes of one pipeline stage (a | b | m buffers)
     uint32_t stages;       // stages in the ring, 2..kMaxStages
+    uint32_t slots;        // gathered-value slots between compute and encoder warps, 1..kMaxSlots
+    uint32_t slot_bytes;   // bytes of one slot
+    uint32_t cv16;         // gathered values stored as 16-bit words (value width <= 16)
+    uint32_t stage_target;          // bytes of input to keep staged ahead (sets the ring depth)
+    uint32_t stage_target_compact;  // ring depth of compacting passes
     uint32_t a_off, b_off, m_off;  // offsets of the buffers inside a stage
+    uint64_t a_stride, b_stride, m_stride;  // bytes per tile when tiles fall on word boundaries, else 0
     uint32_t smem_fixed;           // bytes before the first stage
 };
 

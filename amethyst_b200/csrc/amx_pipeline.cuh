@@ -1,12 +1,12 @@
 // amx_pipeline.cuh -- the tile pipeline kernel behind filter, compressstore, binary ops,
 // conversion, aggregation and fused chains.
 //
-// Persistent CTAs (two per SM) of ten warps with three roles, handing work over through
-// shared-memory mbarriers so that no compute warp ever waits on global-memory latency:
+// Persistent CTAs (one per SM) with three warp roles, handing work over through shared-memory
+// mbarriers so that no compute warp ever waits on global-memory latency:
 //   * the loader warp (one lane) takes tiles from an atomic ticket counter and stages each
-//     tile's bytes of every input into a two-deep ring of shared-memory stages with 1-D bulk
+//     tile's bytes of every input into a ring of 2..8 shared-memory stages with 1-D bulk
 //     copies (cp.async.bulk, completion on the stage's `full` mbarrier);
-//   * eight compute warps decode R elements per thread straight from the staged packed words
+//   * 8 or 16 compute warps decode R elements per thread straight from the staged packed words
 //     (a policy: warp-major runtime-width readers or thread-contiguous compile-time-width
 //     readers), apply the op and the predicate, build the bitmask / aggregate / count, scan the
 //     tile's survivors, publish the count for the decoupled look-back, gather the survivors in
@@ -39,47 +39,63 @@ __device__ __forceinline__ void col_range(const ColDev& c, uint64_t e0, uint64_t
     if (b0 > b1) b0 = b1;
 }
 
-struct Copy {
-    const uint8_t* src;
-    uint8_t* dst;
-    uint32_t bytes;
-};
-
-// Plan the staging of one column: the 16-byte-aligned body goes through the bulk-copy unit;
-// a ragged tail at the very end of the column (< 16 bytes) is copied here with plain loads.
-__device__ __forceinline__ void stage_plan(const ColDev& c, uint64_t e0, uint64_t e1, uint8_t* dst, uint64_t* sbase,
-                                           Copy* cp, int& ncp, uint32_t& tx)
+// Byte range of one column for a tile: tile * stride when every tile of the column covers
+// exactly `stride` bytes (precomputed on the host; 0 when tiles do not fall on word
+// boundaries), else col_range.
+__device__ __forceinline__ void tile_bytes(const ColDev& c, uint64_t stride, uint64_t tile, uint64_t e0, uint64_t e1,
+                                           uint64_t& b0, uint64_t& b1)
 {
-    uint64_t b0, b1;
-    col_range(c, e0, e1, b0, b1);
-    const uint64_t s16 = b0 & ~15ull;
-    *sbase = s16;
-    uint64_t tend = (b1 + 15) & ~15ull;
-    const uint64_t total16 = c.bytes & ~15ull;
-    if (tend > total16) tend = total16;
-    const uint8_t* src = reinterpret_cast<const uint8_t*>(c.data);
-    if (tend > s16) {
-        cp[ncp++] = Copy{src + s16, dst, (uint32_t)(tend - s16)};
-        tx += (uint32_t)(tend - s16);
+    if (stride) {
+        b0 = tile * stride;
+        b1 = b0 + stride;
+        if (b1 > c.bytes) b1 = c.bytes;
+        if (b0 > b1) b0 = b1;
     }
-    for (uint64_t x = tend > s16 ? tend : s16; x < b1; x++) dst[x - s16] = src[x];
+    else {
+        col_range(c, e0, e1, b0, b1);
+    }
 }
 
-// Issue the staging of one tile into stage buffer `st` (one thread).
+// Issue the staging of one tile into stage buffer `st` (one thread): plain scalar code, no
+// arrays, so the loader spends as little time as possible per tile.
 __device__ __forceinline__ void stage_issue(const PipeParams& p, uint8_t* st, uint64_t* sbase, uint64_t* bar,
                                             uint64_t tile, uint32_t tile_elems)
 {
     const uint64_t e0 = tile * tile_elems;
     uint64_t e1 = e0 + tile_elems;
     if (e1 > p.n) e1 = p.n;
-    Copy cp[3];
-    int ncp = 0;
-    uint32_t tx = 0;
-    stage_plan(p.a, e0, e1, st + p.a_off, &sbase[0], cp, ncp, tx);
-    if (p.has_b) stage_plan(p.b, e0, e1, st + p.b_off, &sbase[1], cp, ncp, tx);
-    if (p.has_mask_in) stage_plan(p.m, e0, e1, st + p.m_off, &sbase[2], cp, ncp, tx);
-    mbar_arrive_expect_tx(bar, tx);
-    for (int i = 0; i < ncp; i++) bulk_g2s(cp[i].dst, cp[i].src, cp[i].bytes, bar);
+    uint64_t a0, a1, b0 = 0, b1 = 0, m0 = 0, m1 = 0;
+    tile_bytes(p.a, p.a_stride, tile, e0, e1, a0, a1);
+    if (p.has_b) tile_bytes(p.b, p.b_stride, tile, e0, e1, b0, b1);
+    if (p.has_mask_in) tile_bytes(p.m, p.m_stride, tile, e0, e1, m0, m1);
+    // body of each range through the bulk-copy unit (16-byte aligned), ragged tail by hand
+    const uint64_t as = a0 & ~15ull, bs = b0 & ~15ull, ms = m0 & ~15ull;
+    uint64_t ae = (a1 + 15) & ~15ull, be = (b1 + 15) & ~15ull, me = (m1 + 15) & ~15ull;
+    if (ae > (p.a.bytes & ~15ull)) ae = p.a.bytes & ~15ull;
+    if (be > (p.b.bytes & ~15ull)) be = p.b.bytes & ~15ull;
+    if (me > (p.m.bytes & ~15ull)) me = p.m.bytes & ~15ull;
+    const uint32_t at = ae > as ? (uint32_t)(ae - as) : 0;
+    const uint32_t bt = (p.has_b && be > bs) ? (uint32_t)(be - bs) : 0;
+    const uint32_t mt = (p.has_mask_in && me > ms) ? (uint32_t)(me - ms) : 0;
+    sbase[0] = as;
+    sbase[1] = bs;
+    sbase[2] = ms;
+    if (a1 > (ae > as ? ae : as)) {  // ragged tail at the very end of the column (< 16 bytes)
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(p.a.data);
+        for (uint64_t x = ae > as ? ae : as; x < a1; x++) st[p.a_off + (x - as)] = src[x];
+    }
+    if (p.has_b && b1 > (be > bs ? be : bs)) {
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(p.b.data);
+        for (uint64_t x = be > bs ? be : bs; x < b1; x++) st[p.b_off + (x - bs)] = src[x];
+    }
+    if (p.has_mask_in && m1 > (me > ms ? me : ms)) {
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(p.m.data);
+        for (uint64_t x = me > ms ? me : ms; x < m1; x++) st[p.m_off + (x - ms)] = src[x];
+    }
+    mbar_arrive_expect_tx(bar, at + bt + mt);
+    if (at) bulk_g2s(st + p.a_off, reinterpret_cast<const uint8_t*>(p.a.data) + as, at, bar);
+    if (bt) bulk_g2s(st + p.b_off, reinterpret_cast<const uint8_t*>(p.b.data) + bs, bt, bar);
+    if (mt) bulk_g2s(st + p.m_off, reinterpret_cast<const uint8_t*>(p.m.data) + ms, mt, bar);
 }
 
 // bits [bit, bit+R) of a little-endian uint32 word array (R <= 64)
@@ -199,55 +215,41 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
     }
 }
 
-// Look-back for a tile whose survivor count (AGG) is already published: returns the number
-// of survivors in all earlier tiles and publishes the tile's inclusive prefix (INC).  All 32
-// lanes of one warp call it.  Each round reads 256 predecessor status words at once (8 per
-// lane, independent loads), so one round usually reaches a published prefix.  Every wait is
-// bounded: on timeout the error word is set and the missing value is taken as 0.
+// Sum of the published survivor counts of tiles [lo, hi).  All 32 lanes of one warp call it;
+// each round has 256 status loads in flight (8 per lane).  Waits for counts not yet published
+// are bounded: on timeout the error word is set and the count is taken as 0.
 constexpr int kLookPerLane = 8;
 
-__device__ __forceinline__ uint64_t lookback_prev(uint64_t* status, uint64_t tile, uint64_t agg, uint32_t* err)
+__device__ __forceinline__ uint64_t sum_counts(const uint64_t* status, uint64_t lo, uint64_t hi, uint32_t* err)
 {
     const uint32_t lane = threadIdx.x & 31;
-    if (tile == 0) return 0;  // tile 0 published its inclusive prefix directly
-    uint64_t excl = 0;
-    int64_t j = (int64_t)tile - 1;
-    bool done = false;
-    while (!done) {
+    uint64_t acc = 0;
+    for (uint64_t base = lo; base < hi; base += 32 * kLookPerLane) {
         uint64_t st[kLookPerLane];
 #pragma unroll
-        for (int m = 0; m < kLookPerLane; m++) {  // all loads of the round in flight together
-            const int64_t idx = j - (int64_t)(lane + 32 * m);
-            st[m] = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
+        for (int m = 0; m < kLookPerLane; m++) {
+            const uint64_t idx = base + lane + 32 * m;
+            st[m] = idx < hi ? ld_relaxed_u64(&status[idx]) : kFlagAgg;
         }
-        // consume the window nearest-first, 32 predecessors at a time, and stop at the first
-        // group holding an inclusive prefix: never wait on tiles beyond it
 #pragma unroll
         for (int m = 0; m < kLookPerLane; m++) {
-            if (done) break;
-            const int64_t idx = j - (int64_t)(lane + 32 * m);
+            const uint64_t idx = base + lane + 32 * m;
             uint32_t spins = 0;
-            while ((st[m] >> 62) == 0) {  // an earlier tile still decoding
+            while ((st[m] >> 62) == 0) {  // that tile is still being decoded
                 if (++spins > kWaitSpins) {
                     record_error(err, AMX_ERR_TIMEOUT);
-                    st[m] = kFlagInc;
+                    st[m] = kFlagAgg;
                     break;
                 }
                 if (spins > 8) __nanosleep(20);
                 st[m] = ld_relaxed_u64(&status[idx]);
             }
-            const uint32_t inc = __ballot_sync(0xffffffffu, (st[m] >> 62) == 2);
-            const int first = __ffs(inc) - 1;
-            uint64_t v = (first < 0 || (int)lane <= first) ? (st[m] & kValMask) : 0;
-#pragma unroll
-            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            excl += v;
-            done = first >= 0;
+            acc += st[m] & kValMask;
         }
-        j -= 32 * kLookPerLane;
     }
-    if (lane == 0) st_relaxed_u64(&status[tile], kFlagInc | (excl + agg));
-    return excl;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
@@ -255,9 +257,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ void compute_bar()
+// named barrier 1 over the compute warps only (the loader and look-back warps never join it)
+template <uint32_t N>
+__device__ __forceinline__ void compute_bar_n()
 {
-    asm volatile("bar.sync 1, %0;" ::"n"(kPipeCompute) : "memory");
+    asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory");
 }
 
 __device__ __forceinline__ void wait_or_flag(uint64_t* bar, uint32_t parity, uint32_t* err)
@@ -265,45 +269,77 @@ __device__ __forceinline__ void wait_or_flag(uint64_t* bar, uint32_t parity, uin
     if (!mbar_wait_bounded(bar, parity)) record_error(err, AMX_ERR_TIMEOUT);
 }
 
-// Shared-memory map (dynamic shared memory), for up to kMaxStages stages:
-//   [0,64) full[8]  [64,128) empty[8]  [128,144) agg[2]  [144,160) gready[2]   (mbarriers)
-//   [160,224)  tickets[8]              [224,416) stage base offsets [8][3]
-//   [416,480)  warp totals [2][8]      [480,544) warp counts      [544,592) per-slot tile / total / offset
-//   [608,672)  warp aggregates         [1024,3072) tile bitmap (thread-contiguous policies)
-//   [kCvOff, smem_fixed)  gathered values;  [smem_fixed, ...) p.stages stage buffers
+// Shared-memory map (dynamic shared memory), for up to kMaxStages stages and kMaxSlots slots:
+//   [0,64) full[8]  [64,128) empty[8]  [128,160) agg[4]  [160,192) gready[4]  [192,224) scat[4]
+//   [224,256) cvfree[4]                                                        (mbarriers)
+//   [256,320)  tickets[8]              [320,512) stage base offsets [8][3]
+//   [512,640)  warp totals [2][16]     [640,768) warp counts [16]  [768,848) per-slot tile / total / offset
+//   [896,1024) warp aggregates [16]    [1024,5120) tile bitmap (thread-contiguous policies)
+//   [kCvOff, smem_fixed)  gathered-value slots;  [smem_fixed, ...) p.stages stage buffers
 constexpr uint32_t kBitmapOff = 1024;
-constexpr uint32_t kCvOff = 3072;
+constexpr uint32_t kCvOff = 5120;
 constexpr uint64_t kNoTile = ~0ull;
+constexpr uint32_t kEncoderWarps = 2;
+constexpr int kSparseMax = 3;  // survivors per thread up to which a warp gathers sparsely
+constexpr uint32_t kCtlThreads = 32 * (2 + kEncoderWarps);  // loader + look-back + encoders
+
+// gathered values are kept as 16-bit words when the value width allows it
+template <typename V>
+__device__ __forceinline__ void cv_put(uint8_t* cv, bool cv16, uint32_t i, V x)
+{
+    if (cv16)
+        reinterpret_cast<uint16_t*>(cv)[i] = (uint16_t)x;
+    else
+        reinterpret_cast<V*>(cv)[i] = x;
+}
+
+template <typename V>
+__device__ __forceinline__ void encode_any(const OutDev& o, const uint8_t* cv, bool cv16, uint32_t cnt, uint64_t g,
+                                           bool last, uint32_t tid, uint32_t T)
+{
+    if (cv16)
+        encode_tile<uint16_t>(o, reinterpret_cast<const uint16_t*>(cv), cnt, g, last, tid, T);
+    else
+        encode_tile<V>(o, reinterpret_cast<const V*>(cv), cnt, g, last, tid, T);
+}
 
 template <class Pol>
-__global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(const __grid_constant__ PipeParams p)
+__global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
+    pipe_kernel(const __grid_constant__ PipeParams p)
 {
     using V = typename Pol::V;
     constexpr int R = Pol::R;
     constexpr bool WM = Pol::kWarpMajor;
-    constexpr uint32_t T = kPipeCompute;
+    constexpr uint32_t T = Pol::kCompute;
     constexpr uint32_t NW = T / 32;
     constexpr uint32_t TILE = T * R;
     static_assert(TILE / 32 * 4 <= kCvOff - kBitmapOff, "bitmap region");
+    static_assert(NW <= 16, "warp arrays hold 16 compute warps");
     static_assert(!WM || R <= 32, "warp-major runs keep one ballot per lane");
+    auto compute_bar = []() { compute_bar_n<T>(); };
 
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + kMaxStages;
-    uint64_t* aggb = full + 2 * kMaxStages;
-    uint64_t* gready = aggb + 2;
-    volatile uint64_t* tickets = reinterpret_cast<volatile uint64_t*>(smem + 160);
-    uint64_t* sbase = reinterpret_cast<uint64_t*>(smem + 224);
-    volatile uint32_t* warp_tot = reinterpret_cast<volatile uint32_t*>(smem + 416);
-    uint64_t* warp_cnt = reinterpret_cast<uint64_t*>(smem + 480);
-    volatile uint64_t* slot_tile = reinterpret_cast<volatile uint64_t*>(smem + 544);
-    volatile uint32_t* slot_total = reinterpret_cast<volatile uint32_t*>(smem + 560);
-    volatile uint64_t* slot_g = reinterpret_cast<volatile uint64_t*>(smem + 576);
-    uint64_t* warp_agg = reinterpret_cast<uint64_t*>(smem + 608);
-    const uint32_t S = p.stages;
+    uint64_t* aggb = reinterpret_cast<uint64_t*>(smem + 128);
+    uint64_t* gready = reinterpret_cast<uint64_t*>(smem + 160);
+    uint64_t* scat = reinterpret_cast<uint64_t*>(smem + 192);
+    uint64_t* cvfree = reinterpret_cast<uint64_t*>(smem + 224);
+    volatile uint64_t* tickets = reinterpret_cast<volatile uint64_t*>(smem + 256);
+    uint64_t* sbase = reinterpret_cast<uint64_t*>(smem + 320);
+    volatile uint32_t* warp_tot = reinterpret_cast<volatile uint32_t*>(smem + 512);
+    uint64_t* warp_cnt = reinterpret_cast<uint64_t*>(smem + 640);
+    volatile uint64_t* slot_tile = reinterpret_cast<volatile uint64_t*>(smem + 768);
+    volatile uint32_t* slot_total = reinterpret_cast<volatile uint32_t*>(smem + 800);
+    volatile uint64_t* slot_g = reinterpret_cast<volatile uint64_t*>(smem + 816);
+    uint64_t* warp_agg = reinterpret_cast<uint64_t*>(smem + 896);
     uint32_t* bitmap = reinterpret_cast<uint32_t*>(smem + kBitmapOff);
-    V* cv = reinterpret_cast<V*>(smem + kCvOff);
+    uint8_t* cv = smem + kCvOff;
     uint8_t* stage0 = smem + p.smem_fixed;
+    const uint32_t S = p.stages;
+    const uint32_t NB = p.slots;
+    const bool cv16 = p.cv16 != 0;
+    const bool compact = p.has_out && p.compact;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
@@ -312,9 +348,11 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], NW);
         }
-        for (int q = 0; q < 2; q++) {
+        for (uint32_t q = 0; q < NB; q++) {
             mbar_init(&aggb[q], 1);
             mbar_init(&gready[q], 1);
+            mbar_init(&scat[q], NW);
+            mbar_init(&cvfree[q], kEncoderWarps);
         }
         fence_mbar_init();
     }
@@ -362,19 +400,55 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
         return;
     }
     // ---------------------------------------------------------------- look-back warp
+    // The CTA's tiles arrive in increasing ticket order, so the output offset of a tile is the
+    // end of this CTA's previous tile plus the survivor counts of the tiles in between (other
+    // CTAs publish each count right after the tile's scan).  No tile waits on another tile's
+    // look-back: there is no chain of inclusive prefixes across CTAs.
     if (warp == NW + 1) {
-        if (p.has_out && p.compact) {
-            for (uint32_t j = 0;; j++) {
-                const uint32_t q = j & 1;
-                wait_or_flag(&aggb[q], (j >> 1) & 1, &p.ws->err);
+        if (compact) {
+            uint64_t prev_tile = 0, prev_end = 0;
+            bool first = true;
+            for (uint32_t j = 0, q = 0, ph = 0;; j++) {
+                wait_or_flag(&aggb[q], ph, &p.ws->err);
                 const uint64_t tile = slot_tile[q];
-                if (tile == kNoTile) break;
-                const uint64_t g = lookback_prev(p.status, tile, slot_total[q], &p.ws->err);
-                if (lane == 0) {
-                    slot_g[q] = g;
-                    mbar_arrive(&gready[q]);
+                if (tile != kNoTile) {
+                    const uint64_t lo = first ? 0 : prev_tile + 1;
+                    const uint64_t g = (first ? 0 : prev_end) + sum_counts(p.status, lo, tile, &p.ws->err);
+                    first = false;
+                    prev_tile = tile;
+                    prev_end = g + slot_total[q];
+                    if (lane == 0) slot_g[q] = g;
                 }
                 __syncwarp();
+                if (lane == 0) mbar_arrive(&gready[q]);  // hands the slot to the encoder warps
+                if (tile == kNoTile) break;
+                if (++q == NB) {
+                    q = 0;
+                    ph ^= 1;
+                }
+            }
+        }
+        return;
+    }
+    // ---------------------------------------------------------------- encoder warps
+    // Re-encode each slot's gathered survivors at the offset the look-back warp found, then
+    // give the slot back to the compute warps.
+    if (warp >= NW + 2) {
+        if (compact) {
+            const uint32_t etid = tid - (NW + 2) * 32;
+            for (uint32_t j = 0, q = 0, ph = 0;; j++) {
+                wait_or_flag(&gready[q], ph, &p.ws->err);
+                const uint64_t tile = slot_tile[q];
+                if (tile == kNoTile) break;
+                wait_or_flag(&scat[q], ph, &p.ws->err);  // every compute warp has gathered
+                encode_any<V>(p.out, cv + (size_t)q * p.slot_bytes, cv16, slot_total[q], slot_g[q],
+                              tile == p.num_tiles - 1, etid, 32 * kEncoderWarps);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&cvfree[q]);
+                if (++q == NB) {
+                    q = 0;
+                    ph ^= 1;
+                }
             }
         }
         return;
@@ -382,24 +456,7 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
 
     // ---------------------------------------------------------------- compute warps
     uint64_t my_count = 0, my_agg = 0;
-    bool have_prev = false;
-    uint64_t prev_tile = 0;
-    uint32_t prev_total = 0, prev_j = 0;
-
-    auto finish_prev = [&]() {
-        uint64_t g;
-        if (p.compact) {
-            wait_or_flag(&gready[prev_j & 1], (prev_j >> 1) & 1, &p.ws->err);
-            g = slot_g[prev_j & 1];
-        }
-        else {
-            g = prev_tile * TILE;
-        }
-        encode_tile<V>(p.out, cv, prev_total, g, prev_tile == p.num_tiles - 1, tid, T);
-        compute_bar();  // cv is free
-    };
-
-    uint32_t j = 0, s = 0, sphase = 0;
+    uint32_t j = 0, s = 0, sphase = 0, q = 0, qphase = 0;
     for (;; j++) {
         if (j) {
             if (++s == S) {
@@ -432,8 +489,13 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
                 fl &= bits_at<R>(mw, tid * R);
             }
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
+        // Warp-major runs keep every value in registers and release the stage at once.  The
+        // thread-contiguous (compile-time) policies keep the stage until their survivors are
+        // gathered: a sparse warp re-reads only its few survivors from it.
+        if (WM) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
+        }
 
         if (WM) {
             const uint32_t base = warp * 32 * R + lane;
@@ -452,7 +514,11 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
         }
         if (R < 64) fl &= (1ull << R) - 1;
 
-        if (p.has_agg) {
+        // sparse warp: every thread has at most kSparseMax survivors; the aggregate and the
+        // gather then visit the survivors only (set bits of fl) instead of all R elements
+        const bool sparse = !WM && __all_sync(0xffffffffu, __popcll(fl) <= kSparseMax);
+
+        if (p.has_agg && !sparse) {
             uint64_t a = 0;
             switch (p.agg) {
                 case AMX_AGG_SUM:
@@ -518,7 +584,7 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
 
         if (p.has_out) {
             // block scan: survivors before this thread (or warp) inside the tile
-            volatile uint32_t* wt = warp_tot + 8 * (j & 1);
+            volatile uint32_t* wt = warp_tot + 16 * (j & 1);
             uint32_t pos, total = 0, before = 0;
             if (WM) {
                 if (lane == 0) wt[warp] = c;
@@ -543,33 +609,73 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
                 }
                 pos = before + incl - c;
             }
-            if (p.compact && tid == 0) {
-                st_relaxed_u64(&p.status[tile], (tile == 0 ? kFlagInc : kFlagAgg) | total);
-                slot_tile[j & 1] = tile;
-                slot_total[j & 1] = total;
-                mbar_arrive(&aggb[j & 1]);  // hand the tile to the look-back warp
+            uint8_t* slot = cv;
+            if (compact) {
+                // publish this tile's survivor count for the other CTAs' look-backs at once ...
+                if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
+                // ... but reuse slot q only after the encoder warps are done with its last tile
+                if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
+                if (tid == 0) {
+                    slot_tile[q] = tile;
+                    slot_total[q] = total;
+                    mbar_arrive(&aggb[q]);  // hand the tile to the look-back warp
+                }
+                slot = cv + (size_t)q * p.slot_bytes;
             }
-
-            if (have_prev) finish_prev();  // ends with a compute barrier: cv is free
-
             if (WM) {
                 const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
                 for (int i = 0; i < R; i++) {
-                    if ((fl >> i) & 1) cv[pos + __popc(bal[i] & lt)] = v[i];
+                    if ((fl >> i) & 1) cv_put<V>(slot, cv16, pos + __popc(bal[i] & lt), v[i]);
                     pos += __popc(bal[i]);
                 }
             }
+            else if (sparse) {
+                uint64_t a = 0;
+                for (uint64_t f = fl; f; f &= f - 1) {
+                    const V x = Pol::value_at(p, st, sbase + 3 * s, e0, __ffsll((long long)f) - 1);
+                    cv_put<V>(slot, cv16, pos++, x);
+                    a = agg_combine(p.agg, a, agg_encode(p.agg, (uint64_t)x));
+                }
+                if (p.has_agg) my_agg = agg_combine(p.agg, my_agg, a);
+            }
+            else if (cv16) {
+                uint16_t* dst = reinterpret_cast<uint16_t*>(slot) + pos;
+#pragma unroll
+                for (int i = 0; i < R; i++)
+                    if ((fl >> i) & 1) *dst++ = (uint16_t)v[i];
+            }
             else {
-                V* dst = cv + pos;
+                V* dst = reinterpret_cast<V*>(slot) + pos;
 #pragma unroll
                 for (int i = 0; i < R; i++)
                     if ((fl >> i) & 1) *dst++ = v[i];
             }
-            have_prev = true;
-            prev_tile = tile;
-            prev_total = total;
-            prev_j = j;
+            if (compact) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&scat[q]);  // this warp's survivors are in slot q
+                if (++q == NB) {
+                    q = 0;
+                    qphase ^= 1;
+                }
+            }
+            else {  // element-wise output: the offset is known, encode right away
+                compute_bar();
+                encode_any<V>(p.out, cv, cv16, total, e0, tile == p.num_tiles - 1, tid, T);
+                compute_bar();
+            }
+        }
+        if (!WM) {
+            if (!p.has_out && p.has_agg && sparse) {
+                uint64_t a = 0;
+                for (uint64_t f = fl; f; f &= f - 1) {
+                    const V x = Pol::value_at(p, st, sbase + 3 * s, e0, __ffsll((long long)f) - 1);
+                    a = agg_combine(p.agg, a, agg_encode(p.agg, (uint64_t)x));
+                }
+                my_agg = agg_combine(p.agg, my_agg, a);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
         }
         if (!WM && p.mask_out) {
             compute_bar();
@@ -581,11 +687,13 @@ __global__ void __launch_bounds__(kPipeThreads, Pol::kMinBlocks) pipe_kernel(con
             compute_bar();
         }
     }
-    if (p.has_out && p.compact && tid == 0) {  // release the look-back warp
-        slot_tile[j & 1] = kNoTile;
-        mbar_arrive(&aggb[j & 1]);
+    if (compact) {  // release the look-back and encoder warps through the next free slot
+        if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
+        if (tid == 0) {
+            slot_tile[q] = kNoTile;
+            mbar_arrive(&aggb[q]);
+        }
     }
-    if (have_prev) finish_prev();
 
     // CTA totals -> workspace; the last CTA to finish publishes the scalar results
 #pragma unroll
@@ -696,8 +804,9 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
 // Any formats and widths: warp-major runtime readers, 64-bit values, 16 elements per thread.
 struct GenericPol {
     using V = uint64_t;
-    static constexpr int R = 16;
+    static constexpr int R = 8;
     static constexpr bool kWarpMajor = true;
+    static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
@@ -727,6 +836,12 @@ struct GenericPol {
             }
         }
         finish_values<R, V>(p, v, fl);
+    }
+
+    // warp-major runs never take the sparse path (their values stay in registers)
+    __device__ __forceinline__ static V value_at(const PipeParams&, const uint8_t*, const uint64_t*, uint64_t, int)
+    {
+        return 0;
     }
 };
 

@@ -97,7 +97,10 @@ struct SlabPol {
     static constexpr int SPT = EPS >= 32 ? 1 : 32 / EPS;
     static constexpr int R = EPS * SPT;
     static constexpr bool kWarpMajor = false;
-    static constexpr int kMinBlocks = R > 40 ? 1 : 2;
+    // one CTA per SM: 16 compute warps, or 8 for the register-heavy 64-element runs and for
+    // widths >= 17 (10+ slabs per thread: a 16-warp tile would not fit twice in shared memory)
+    static constexpr uint32_t kCompute = (R > 40 || B >= 17) ? 256 : 512;
+    static constexpr int kMinBlocks = 1;
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
                                                   uint64_t e0, V (&v)[R], uint64_t& fl)
@@ -108,6 +111,18 @@ struct SlabPol {
         lds_words<SPT>(w, s);
         unpack_slabs<B, EPS, SPT, R>(s, v);
         finish32<R>(p, v, fl);
+    }
+
+    // value of element i of this thread's run, re-read from the staged words (sparse gather)
+    __device__ __forceinline__ static V value_at(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
+                                                 uint64_t e0, int i)
+    {
+        const uint64_t first = e0 + threadIdx.x * R;
+        const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first / EPS - sb[0] / 8);
+        const uint32_t j = (uint32_t)i / EPS, k = (uint32_t)i - j * EPS;
+        uint32_t x = (uint32_t)((w[j] >> (k * B)) & ((1ull << B) - 1));
+        if (p.need_vmask) x &= (uint32_t)p.vmask;
+        return x;
     }
 };
 
@@ -132,7 +147,8 @@ struct Slab2Pol {
     static constexpr int SA = R / EA;
     static constexpr int SB = R / EB;
     static constexpr bool kWarpMajor = false;
-    static constexpr int kMinBlocks = R > 40 ? 1 : 2;
+    static constexpr uint32_t kCompute = R > 40 ? 256 : 512;
+    static constexpr int kMinBlocks = 1;
     static_assert(R <= 64, "run too long for the flag word");
 
     __device__ __forceinline__ static void decode(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
@@ -161,6 +177,32 @@ struct Slab2Pol {
             }
         }
         finish32<R>(p, v, fl);
+    }
+
+    // value of element i of this thread's run, re-read from the staged words (sparse gather)
+    __device__ __forceinline__ static V value_at(const PipeParams& p, const uint8_t* st, const uint64_t* sb,
+                                                 uint64_t e0, int i)
+    {
+        const uint64_t first = e0 + threadIdx.x * R;
+        const uint64_t* wa = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first / EA - sb[0] / 8);
+        const uint64_t* wb = reinterpret_cast<const uint64_t*>(st + p.b_off) + (first / EB - sb[1] / 8);
+        const uint32_t ja = (uint32_t)i / EA, ka = (uint32_t)i - ja * EA;
+        const uint32_t jb = (uint32_t)i / EB, kb = (uint32_t)i - jb * EB;
+        const uint32_t a = (uint32_t)((wa[ja] >> (ka * BA)) & ((1ull << BA) - 1));
+        const uint32_t b = (uint32_t)((wb[jb] >> (kb * BB)) & ((1ull << BB) - 1));
+        uint32_t x;
+        switch (p.op) {
+            case AMX_OP_ADD: x = a + b; break;
+            case AMX_OP_SUB: x = a - b; break;
+            case AMX_OP_MUL: x = a * b; break;
+            case AMX_OP_MIN: x = a < b ? a : b; break;
+            case AMX_OP_MAX: x = a > b ? a : b; break;
+            case AMX_OP_AND: x = a & b; break;
+            case AMX_OP_OR: x = a | b; break;
+            default: x = a ^ b; break;
+        }
+        if (p.need_vmask) x &= (uint32_t)p.vmask;
+        return x;
     }
 };
 
