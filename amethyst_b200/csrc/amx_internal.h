@@ -94,6 +94,22 @@ struct PipeParams {
     uint32_t a_off, b_off, m_off;  // offsets of the buffers inside a stage
     uint64_t a_stride, b_stride, m_stride;  // bytes per tile when tiles fall on word boundaries, else 0
     uint32_t smem_fixed;           // bytes before the first stage
+    // field-parallel predicate of the slab-word policies (SwarPol): the passing field values
+    // form the interval [lo, hi1) or its complement; sw_l1 / sw_l2 are lo and hi1 repeated in
+    // every field with the field's top bit cleared, sw_h has the top bit of every field set
+    uint32_t sw_mode;  // kSw* bits
+    uint32_t sw_pad;
+    uint64_t sw_h;
+    uint64_t sw_l1;
+    uint64_t sw_l2;
 };
+
+// SwarPol predicate modes
+constexpr uint32_t kSwLo = 1;      // test v >= lo
+constexpr uint32_t kSwHi = 2;      // test v < hi1
+constexpr uint32_t kSwLoTop = 4;   // top bit of lo's field
+constexpr uint32_t kSwHiTop = 8;   // top bit of hi1's field
+constexpr uint32_t kSwNeg = 16;    // complement the result
+constexpr uint32_t kSwNone = 32;   // no value passes (before the complement)
 
 }  // namespace amx

@@ -19,6 +19,7 @@
 #pragma once
 
 #include "amx_device.cuh"
+#include "amx_swar.cuh"
 
 namespace amx {
 
@@ -215,6 +216,53 @@ __device__ __forceinline__ void encode_tile(const OutDev& o, const V* cv, uint32
     }
 }
 
+// encode_tile for a slab output whose width OB is known at compile time: 32-bit tile-local
+// indices, unrolled field loads, and a division by a constant.  Same ownership rules.
+template <int OB, typename V>
+__device__ __forceinline__ void encode_slab_ct(const OutDev& o, const V* cv, uint32_t cnt, uint64_t g, bool last,
+                                               uint32_t tid, uint32_t T)
+{
+    constexpr int EPS = 64 / OB;
+    constexpr uint64_t M = (1ull << OB) - 1;
+    constexpr uint64_t LIVE = EPS * OB >= 64 ? ~0ull : ((1ull << (EPS * OB)) - 1);
+    unsigned long long* out = reinterpret_cast<unsigned long long*>(o.data);
+    if (cnt) {
+        const uint64_t w0 = g / EPS;
+        const uint32_t nw = (uint32_t)((g + cnt - 1) / EPS - w0 + 1);
+        const int32_t r00 = (int32_t)(int64_t)(w0 * EPS - g);  // in (-EPS, 0]
+        for (uint32_t i = tid; i < nw; i += T) {
+            const int32_t r0 = r00 + (int32_t)(i * EPS);
+            uint64_t acc = 0;
+            if (r0 >= 0 && r0 + EPS <= (int32_t)cnt) {
+                const V* c = cv + r0;
+#pragma unroll
+                for (int k = 0; k < EPS; k++) acc |= ((uint64_t)c[k] & M) << (k * OB);
+                out[w0 + i] = acc;
+            }
+            else {
+                uint64_t own = 0;
+#pragma unroll
+                for (int k = 0; k < EPS; k++) {
+                    const int32_t r = r0 + k;
+                    if (r >= 0 && r < (int32_t)cnt) {
+                        acc |= ((uint64_t)cv[r] & M) << (k * OB);
+                        own |= M << (k * OB);
+                    }
+                }
+                if (r0 + EPS - 1 < (int32_t)cnt && r0 + EPS - 1 >= 0) own |= ~LIVE;
+                atomicAnd(&out[w0 + i], ~own);
+                atomicOr(&out[w0 + i], acc);
+            }
+        }
+    }
+    if (last && tid == 0) {
+        const uint64_t total = g + cnt;
+        const uint64_t tw = total / EPS;
+        const uint32_t k = (uint32_t)(total - tw * EPS);
+        if (k) atomicAnd(&out[tw], (1ull << (k * OB)) - 1);
+    }
+}
+
 // Sum of the published survivor counts of tiles [lo, hi).  All 32 lanes of one warp call it;
 // each round has 256 status loads in flight (8 per lane).  Waits for counts not yet published
 // are bounded: on timeout the error word is set and the count is taken as 0.
@@ -279,7 +327,7 @@ __device__ __forceinline__ void wait_or_flag(uint64_t* bar, uint32_t parity, uin
 constexpr uint32_t kBitmapOff = 1024;
 constexpr uint32_t kCvOff = 5120;
 constexpr uint64_t kNoTile = ~0ull;
-constexpr uint32_t kEncoderWarps = 2;
+constexpr uint32_t kEncoderWarps = 4;
 constexpr int kSparseMax = 3;  // survivors per thread up to which a warp gathers sparsely
 constexpr uint32_t kCtlThreads = 32 * (2 + kEncoderWarps);  // loader + look-back + encoders
 
@@ -441,8 +489,25 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 const uint64_t tile = slot_tile[q];
                 if (tile == kNoTile) break;
                 wait_or_flag(&scat[q], ph, &p.ws->err);  // every compute warp has gathered
-                encode_any<V>(p.out, cv + (size_t)q * p.slot_bytes, cv16, slot_total[q], slot_g[q],
-                              tile == p.num_tiles - 1, etid, 32 * kEncoderWarps);
+                const uint8_t* sv = cv + (size_t)q * p.slot_bytes;
+                bool done = false;
+                if constexpr (Pol::kSwar) {
+                    // the usual compressstore: slabs of the input width in, slabs of it out
+                    if (p.out.format == AMX_SLAB && p.out.bits == (uint32_t)Pol::kBits) {
+                        if (cv16)
+                            encode_slab_ct<Pol::kBits, uint16_t>(p.out, reinterpret_cast<const uint16_t*>(sv),
+                                                                slot_total[q], slot_g[q], tile == p.num_tiles - 1,
+                                                                etid, 32 * kEncoderWarps);
+                        else
+                            encode_slab_ct<Pol::kBits, uint32_t>(p.out, reinterpret_cast<const uint32_t*>(sv),
+                                                                slot_total[q], slot_g[q], tile == p.num_tiles - 1,
+                                                                etid, 32 * kEncoderWarps);
+                        done = true;
+                    }
+                }
+                if (!done)
+                    encode_any<V>(p.out, sv, cv16, slot_total[q], slot_g[q], tile == p.num_tiles - 1, etid,
+                                  32 * kEncoderWarps);
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&cvfree[q]);
                 if (++q == NB) {
@@ -457,6 +522,130 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     // ---------------------------------------------------------------- compute warps
     uint64_t my_count = 0, my_agg = 0;
     uint32_t j = 0, s = 0, sphase = 0, q = 0, qphase = 0;
+    if constexpr (Pol::kSwar) {
+        // Field-parallel path (one slab column, a predicate, no input mask): the flags are
+        // computed on whole slab words, the stage is released as soon as the thread's words are
+        // in registers, and only the passing fields are ever extracted.
+        constexpr int B = Pol::kBits;
+        constexpr int EPS = Pol::EPS;
+        constexpr int SPT = Pol::SPT;
+        for (;; j++) {
+            if (j) {
+                if (++s == S) {
+                    s = 0;
+                    sphase ^= 1;
+                }
+            }
+            wait_or_flag(&full[s], sphase, &p.ws->err);
+            const uint64_t tile = tickets[s];
+            if (tile >= p.num_tiles) break;
+            const uint64_t e0 = tile * TILE;
+            const uint64_t rem = p.n - e0;
+            const uint32_t valid = rem < TILE ? (uint32_t)rem : TILE;
+            uint64_t x[SPT];
+            {
+                const uint8_t* st = stage0 + s * p.stage_bytes;
+                const uint64_t first = tile * (uint64_t)(T * SPT) + tid * SPT;  // first slab of this thread
+                lds_words<SPT>(reinterpret_cast<const uint64_t*>(st + p.a_off) + (first - sbase[3 * s] / 8), x);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);  // the words are in registers: stage s is free
+
+            uint64_t g[SPT];
+            swar_flags<B, SPT>(p.sw_mode, x, g, p.sw_l1, p.sw_l2);
+            const uint32_t le0 = tid * R;
+            if (le0 + R > valid) {  // elements past the column's end do not pass
+#pragma unroll
+                for (int i = 0; i < SPT; i++) {
+                    const int left = (int)valid - (int)(le0 + i * EPS);
+                    g[i] &= left <= 0 ? 0ull : (left >= EPS ? ~0ull : ((1ull << (left * B)) - 1));
+                }
+            }
+            uint32_t c = 0;
+#pragma unroll
+            for (int i = 0; i < SPT; i++) c += __popcll(g[i]);
+            my_count += c;
+
+            if (p.mask_out) {
+                uint64_t fl = 0;
+#pragma unroll
+                for (int i = 0; i < SPT; i++)
+#pragma unroll
+                    for (int k = 0; k < EPS; k++) fl |= ((g[i] >> (k * B + B - 1)) & 1ull) << (i * EPS + k);
+                if (fl) {
+                    const uint32_t wi = le0 >> 5, sh = le0 & 31;
+                    atomicOr(&bitmap[wi], (uint32_t)(fl << sh));
+                    if (sh + R > 32) atomicOr(&bitmap[wi + 1], (uint32_t)(fl >> (32 - sh)));
+                    if (sh + R > 64) atomicOr(&bitmap[wi + 2], (uint32_t)(fl >> (64 - sh)));
+                }
+            }
+
+            uint32_t pos = 0;
+            uint8_t* slot = cv;
+            if (p.has_out) {  // compacting: block scan, publish, hand the tile to the look-back
+                volatile uint32_t* wt = warp_tot + 16 * (j & 1);
+                const uint32_t incl = warp_incl_scan<uint32_t>(c);
+                if (lane == 31) wt[warp] = incl;
+                compute_bar();
+                uint32_t total = 0, before = 0;
+#pragma unroll
+                for (uint32_t w = 0; w < NW; w++) {
+                    const uint32_t xw = wt[w];
+                    before += w < warp ? xw : 0;
+                    total += xw;
+                }
+                pos = before + incl - c;
+                if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
+                if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
+                if (tid == 0) {
+                    slot_tile[q] = tile;
+                    slot_total[q] = total;
+                    mbar_arrive(&aggb[q]);
+                }
+                slot = cv + (size_t)q * p.slot_bytes;
+            }
+            if (p.has_out || p.has_agg) {
+                const bool dense = __any_sync(0xffffffffu, 5 * c > 2 * (uint32_t)R);
+                uint64_t a = 0;
+                if (p.has_out) {
+                    if (cv16) {
+                        if (p.has_agg)
+                            swar_visit<B, SPT, uint16_t, true, true>(x, g, dense, reinterpret_cast<uint16_t*>(slot), pos, p.agg, a);
+                        else
+                            swar_visit<B, SPT, uint16_t, true, false>(x, g, dense, reinterpret_cast<uint16_t*>(slot), pos, p.agg, a);
+                    }
+                    else {
+                        if (p.has_agg)
+                            swar_visit<B, SPT, uint32_t, true, true>(x, g, dense, reinterpret_cast<uint32_t*>(slot), pos, p.agg, a);
+                        else
+                            swar_visit<B, SPT, uint32_t, true, false>(x, g, dense, reinterpret_cast<uint32_t*>(slot), pos, p.agg, a);
+                    }
+                }
+                else {
+                    swar_visit<B, SPT, uint32_t, false, true>(x, g, dense, nullptr, 0, p.agg, a);
+                }
+                if (p.has_agg) my_agg = agg_combine(p.agg, my_agg, a);
+            }
+            if (p.has_out) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&scat[q]);  // this warp's survivors are in slot q
+                if (++q == NB) {
+                    q = 0;
+                    qphase ^= 1;
+                }
+            }
+            if (p.mask_out) {
+                compute_bar();
+                const uint32_t words = (valid + 31) / 32;
+                for (uint32_t i = tid; i < words; i += T) {
+                    p.mask_out[e0 / 32 + i] = bitmap[i];
+                    bitmap[i] = 0;
+                }
+                compute_bar();
+            }
+        }
+    }
+    else {
     for (;; j++) {
         if (j) {
             if (++s == S) {
@@ -687,6 +876,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             compute_bar();
         }
     }
+    }
     if (compact) {  // release the look-back and encoder warps through the next free slot
         if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
         if (tid == 0) {
@@ -806,6 +996,7 @@ struct GenericPol {
     using V = uint64_t;
     static constexpr int R = 8;
     static constexpr bool kWarpMajor = true;
+    static constexpr bool kSwar = false;
     static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;
 

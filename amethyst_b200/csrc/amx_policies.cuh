@@ -23,25 +23,6 @@ struct ct_gcd<A, 0> {
     static constexpr int value = A;
 };
 
-// load N consecutive 64-bit words from shared memory, 16 bytes at a time when aligned
-template <int N>
-__device__ __forceinline__ void lds_words(const uint64_t* src, uint64_t (&w)[N])
-{
-    if constexpr (N % 2 == 0) {
-        const uint4* s = reinterpret_cast<const uint4*>(src);
-#pragma unroll
-        for (int i = 0; i < N / 2; i++) {
-            const uint4 x = s[i];
-            w[2 * i] = ((uint64_t)x.y << 32) | x.x;
-            w[2 * i + 1] = ((uint64_t)x.w << 32) | x.z;
-        }
-    }
-    else {
-#pragma unroll
-        for (int i = 0; i < N; i++) w[i] = src[i];
-    }
-}
-
 template <int B, int K>
 __device__ __forceinline__ uint32_t field(uint64_t slab)
 {
@@ -97,6 +78,7 @@ struct SlabPol {
     static constexpr int SPT = EPS >= 32 ? 1 : 32 / EPS;
     static constexpr int R = EPS * SPT;
     static constexpr bool kWarpMajor = false;
+    static constexpr bool kSwar = false;
     // one CTA per SM: 16 compute warps, or 8 for the register-heavy 64-element runs and for
     // widths >= 17 (10+ slabs per thread: a 16-warp tile would not fit twice in shared memory)
     static constexpr uint32_t kCompute = (R > 40 || B >= 17) ? 256 : 512;
@@ -147,6 +129,7 @@ struct Slab2Pol {
     static constexpr int SA = R / EA;
     static constexpr int SB = R / EB;
     static constexpr bool kWarpMajor = false;
+    static constexpr bool kSwar = false;
     static constexpr uint32_t kCompute = R > 40 ? 256 : 512;
     static constexpr int kMinBlocks = 1;
     static_assert(R <= 64, "run too long for the flag word");
@@ -206,7 +189,8 @@ struct Slab2Pol {
     }
 };
 
-// Policy ids: 0 generic, 1..32 SlabPol<B>, 100+ Slab2Pol pairs.
+// Policy ids: 0 generic, 1..32 SlabPol<B>, 100+ Slab2Pol pairs, 201..232 SwarPol<B>.
+constexpr int kSwarPolicyBase = 200;
 #define AMX_SLAB2_PAIRS(X) X(100, 7, 13) X(101, 13, 7) X(102, 11, 11) X(103, 13, 13)
 
 #define AMX_POLICY_LIST(X)                                                                                             \
@@ -219,27 +203,39 @@ struct Slab2Pol {
     X(100, AMX_PAIR(7, 13)) X(101, AMX_PAIR(13, 7)) X(102, AMX_PAIR(11, 11)) X(103, AMX_PAIR(13, 13))
 #define AMX_PAIR(a, b) Slab2Pol<a, b>
 
-// Policy for a request: compile-time widths when every input is a slab column of width
-// <= 32 and values fit 32 bits, else the generic runtime-width policy.  `force` >= 0
-// selects a policy directly (the autotuner and the tests); an inapplicable force falls back
-// to the automatic choice.
+// A request the field-parallel slab policy (SwarPol) serves: one slab column of width <= 32, a
+// predicate on the field values themselves, no input mask, and a compacted output or none.
+inline bool swar_applicable(const PipeParams& p)
+{
+    return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && p.has_pred && !p.has_mask_in &&
+           (!p.has_out || p.compact) && p.op == AMX_OP_LHS && !p.need_vmask && p.vbits <= 32;
+}
+
+// Policy for a request: the field-parallel policy when it applies, else compile-time widths
+// when every input is a slab column of width <= 32 and values fit 32 bits, else the generic
+// runtime-width policy.  `force` >= 0 selects a policy directly (the autotuner and the tests);
+// an inapplicable force falls back to the automatic choice.
 inline int choose_policy(const PipeParams& p, int force)
 {
     const bool v32 = p.vbits <= 32;
     const bool a_slab = p.a.format == AMX_SLAB && p.a.bits <= 32;
+    const bool swar = swar_applicable(p);
     int auto_id = 0;
-    if (v32 && a_slab && !p.has_b) auto_id = (int)p.a.bits;
+    int slab_id = -1;
+    if (v32 && a_slab && !p.has_b) slab_id = (int)p.a.bits;
     // two-column compile-time policies cover the 32-bit-exact ops; the rest take the generic path
     const bool cheap_op = p.op == AMX_OP_ADD || p.op == AMX_OP_SUB || p.op == AMX_OP_MUL || p.op == AMX_OP_MIN ||
                           p.op == AMX_OP_MAX || p.op == AMX_OP_AND || p.op == AMX_OP_OR || p.op == AMX_OP_XOR;
     if (v32 && a_slab && p.has_b && p.b.format == AMX_SLAB && cheap_op) {
 #define AMX_PAIR_MATCH(id, x, y) \
-    if (p.a.bits == x && p.b.bits == y) auto_id = id;
+    if (p.a.bits == x && p.b.bits == y) slab_id = id;
         AMX_SLAB2_PAIRS(AMX_PAIR_MATCH)
 #undef AMX_PAIR_MATCH
     }
+    if (slab_id > 0) auto_id = slab_id;
+    if (swar) auto_id = kSwarPolicyBase + (int)p.a.bits;
     if (force == 0) return 0;
-    if (force > 0 && force == auto_id) return force;
+    if (force > 0 && (force == slab_id || (swar && force == kSwarPolicyBase + (int)p.a.bits))) return force;
     return auto_id;
 }
 

@@ -1,0 +1,149 @@
+// amx_swar.cuh -- field-parallel ("SIMD within a register") predicates on slab words.
+//
+// A slab word holds eps = floor(64/B) fields of B bits.  Instead of extracting every field and
+// comparing it, one 64-bit subtraction compares all fields of a word with a constant at once:
+//
+//   H  = the top bit of every field,  LM = the other B-1 bits of every field,
+//   t  = (x | H) - (rep(c) & LM)       per field: (x_low + 2^(B-1)) - c_low, never borrows
+//                                      across fields, and its top bit is [x_low >= c_low];
+//   ge = (c_top ? x & t : x | t) & H   top bit of every field = [x >= c]
+//
+// so a predicate costs a handful of integer instructions per word instead of per element.
+// The flags stay in place (bit k*B+B-1 of g = element k of the word passes); counting is a
+// popcount, and survivors are read back from the word they came from.  The predicate is
+// turned into an interval of passing values (or its complement) on the host.
+//
+// The reference evaluates the predicate element by element after unpacking each field
+// (src/kernels/filter_slabs.cuh:31-55, get_element in src/common_code.cuh:43-50).
+#pragma once
+
+#include "amx_device.cuh"
+
+namespace amx {
+
+// load N consecutive 64-bit words from shared memory, 16 bytes at a time when aligned
+template <int N>
+__device__ __forceinline__ void lds_words(const uint64_t* src, uint64_t (&w)[N])
+{
+    if constexpr (N % 2 == 0) {
+        const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+        for (int i = 0; i < N / 2; i++) {
+            const uint4 x = s[i];
+            w[2 * i] = ((uint64_t)x.y << 32) | x.x;
+            w[2 * i + 1] = ((uint64_t)x.w << 32) | x.z;
+        }
+    }
+    else {
+#pragma unroll
+        for (int i = 0; i < N; i++) w[i] = src[i];
+    }
+}
+
+// the top bit of each of the floor(64/b) fields of a slab word
+__host__ __device__ constexpr uint64_t swar_top_bits(int b)
+{
+    uint64_t h = 0;
+    for (int k = 0; k < 64 / b; k++) h |= 1ull << (k * b + b - 1);
+    return h;
+}
+
+// One slab column of width B with a predicate, evaluated field-parallel.  Each compute thread
+// owns SPT consecutive slabs of a tile (R = SPT * eps elements, R <= 64).
+template <int B>
+struct SwarPol {
+    using V = uint32_t;
+    static constexpr int kBits = B;
+    static constexpr int EPS = 64 / B;
+    static constexpr int SPT = EPS >= 64 ? 1 : (64 / EPS < 8 ? 64 / EPS : 8);
+    static constexpr int R = EPS * SPT;
+    static constexpr bool kWarpMajor = false;
+    static constexpr bool kSwar = true;
+    static constexpr uint32_t kCompute = 512;
+    static constexpr int kMinBlocks = 1;
+    static constexpr uint64_t kField = (1ull << B) - 1;  // one field
+    static constexpr uint64_t kTop = swar_top_bits(B);    // the top bit of every field
+    static_assert(R <= 64, "a thread's run must fit one 64-bit flag word");
+};
+
+// g[i] = in-place flags of word x[i] for the interval test selected by the template flags
+template <int B, int N, bool LO, bool HI, bool LOTOP, bool HITOP>
+__device__ __forceinline__ void swar_flags_t(const uint64_t (&x)[N], uint64_t (&g)[N], uint64_t l1, uint64_t l2)
+{
+    constexpr uint64_t H = SwarPol<B>::kTop;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const uint64_t xh = x[i] | H;
+        uint64_t f = H;
+        if (LO) {
+            const uint64_t t = xh - l1;
+            f = LOTOP ? (x[i] & t & H) : ((x[i] | t) & H);
+        }
+        if (HI) {
+            const uint64_t t = xh - l2;
+            const uint64_t ge = HITOP ? (x[i] & t) : (x[i] | t);
+            f &= ~ge;
+        }
+        g[i] = f;
+    }
+}
+
+template <int B, int N>
+__device__ __forceinline__ void swar_flags(uint32_t mode, const uint64_t (&x)[N], uint64_t (&g)[N], uint64_t l1,
+                                           uint64_t l2)
+{
+    constexpr uint64_t H = SwarPol<B>::kTop;
+    switch (mode & 15) {
+#define AMX_SW_CASE(m) \
+    case m: swar_flags_t<B, N, (m & 1) != 0, (m & 2) != 0, (m & 4) != 0, (m & 8) != 0>(x, g, l1, l2); break;
+        AMX_SW_CASE(0) AMX_SW_CASE(1) AMX_SW_CASE(2) AMX_SW_CASE(3) AMX_SW_CASE(5) AMX_SW_CASE(7) AMX_SW_CASE(10)
+        AMX_SW_CASE(11) AMX_SW_CASE(15)
+#undef AMX_SW_CASE
+        default:  // unreachable: a top flag is only set together with its test
+#pragma unroll
+            for (int i = 0; i < N; i++) g[i] = 0;
+            break;
+    }
+    if (mode & kSwNone) {
+#pragma unroll
+        for (int i = 0; i < N; i++) g[i] = 0;
+    }
+    if (mode & kSwNeg) {
+#pragma unroll
+        for (int i = 0; i < N; i++) g[i] ^= H;
+    }
+}
+
+// Visit the passing elements of a thread's run in element order: store each value to dst[pos++]
+// (when DST) and fold it into the aggregate `a` (when AGG).  Dense warps walk every field with a
+// predicated store; sparse warps walk the set flag bits only.
+template <int B, int N, typename D, bool DST, bool AGG>
+__device__ __forceinline__ void swar_visit(const uint64_t (&x)[N], const uint64_t (&g)[N], bool dense, D* dst,
+                                           uint32_t pos, uint32_t agg, uint64_t& a)
+{
+    constexpr int EPS = SwarPol<B>::EPS;
+    constexpr uint64_t FM = SwarPol<B>::kField;
+    if (dense) {
+#pragma unroll
+        for (int i = 0; i < N; i++)
+#pragma unroll
+            for (int k = 0; k < EPS; k++)
+                if ((g[i] >> (k * B + B - 1)) & 1) {
+                    const uint32_t v = (uint32_t)((x[i] >> (k * B)) & FM);
+                    if (DST) dst[pos++] = (D)v;
+                    if (AGG) a = agg_combine(agg, a, agg_encode(agg, v));
+                }
+    }
+    else {
+#pragma unroll
+        for (int i = 0; i < N; i++)
+            for (uint64_t f = g[i]; f; f &= f - 1) {
+                const int bp = __ffsll((long long)f) - 1;
+                const uint32_t v = (uint32_t)((x[i] >> (bp - (B - 1))) & FM);
+                if (DST) dst[pos++] = (D)v;
+                if (AGG) a = agg_combine(agg, a, agg_encode(agg, v));
+            }
+    }
+}
+
+}  // namespace amx

@@ -1,0 +1,21 @@
+// amx_swar_w0.cu -- pipe_kernel<SwarPol<B>> for slab widths B = 1..8.
+#include "amx_launch.cuh"
+
+namespace amx {
+
+template <int B>
+amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
+{
+    return launch<SwarPol<B>>(p, ws, ws_bytes, stream);
+}
+
+template amx_status launch_swar_w<1>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<2>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<3>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<4>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<5>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<6>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<7>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<8>(PipeParams&, void*, size_t, cudaStream_t);
+
+}  // namespace amx

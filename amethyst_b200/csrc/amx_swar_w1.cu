@@ -1,0 +1,21 @@
+// amx_swar_w1.cu -- pipe_kernel<SwarPol<B>> for slab widths B = 9..16.
+#include "amx_launch.cuh"
+
+namespace amx {
+
+template <int B>
+amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
+{
+    return launch<SwarPol<B>>(p, ws, ws_bytes, stream);
+}
+
+template amx_status launch_swar_w<9>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<10>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<11>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<12>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<13>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<14>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<15>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<16>(PipeParams&, void*, size_t, cudaStream_t);
+
+}  // namespace amx

@@ -1,0 +1,21 @@
+// amx_swar_w2.cu -- pipe_kernel<SwarPol<B>> for slab widths B = 17..24.
+#include "amx_launch.cuh"
+
+namespace amx {
+
+template <int B>
+amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
+{
+    return launch<SwarPol<B>>(p, ws, ws_bytes, stream);
+}
+
+template amx_status launch_swar_w<17>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<18>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<19>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<20>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<21>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<22>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<23>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<24>(PipeParams&, void*, size_t, cudaStream_t);
+
+}  // namespace amx

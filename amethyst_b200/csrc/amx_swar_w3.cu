@@ -1,0 +1,21 @@
+// amx_swar_w3.cu -- pipe_kernel<SwarPol<B>> for slab widths B = 25..32.
+#include "amx_launch.cuh"
+
+namespace amx {
+
+template <int B>
+amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
+{
+    return launch<SwarPol<B>>(p, ws, ws_bytes, stream);
+}
+
+template amx_status launch_swar_w<25>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<26>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<27>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<28>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<29>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<30>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<31>(PipeParams&, void*, size_t, cudaStream_t);
+template amx_status launch_swar_w<32>(PipeParams&, void*, size_t, cudaStream_t);
+
+}  // namespace amx

@@ -1,0 +1,106 @@
+"""The field-parallel slab policy (whole-word predicate evaluation) against the C oracle,
+bit-exact, for every slab width 1..32 and for predicates at the edges of the value range
+(empty, full, wrap-around and complemented intervals).  Each case runs with the policy forced
+and with the automatic choice, through the C ABI."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import SLAB, gpu_bytes, make_column, to_gpu
+
+pytestmark = pytest.mark.gpu
+
+SWAR_BASE = 200
+
+
+def edge_preds(bits):
+    from amethyst_b200 import _capi as A
+
+    top = (1 << bits) - 1
+    half = 1 << (bits - 1)
+    return [
+        (A.PRED_LT, max(1, top // 10), 0),
+        (A.PRED_LT, 0, 0),                  # nothing passes
+        (A.PRED_LE, top, 0),                # everything passes
+        (A.PRED_GE, half, 0),               # lower bound on the field's top bit
+        (A.PRED_GE, half - 1 if half > 1 else 1, 0),
+        (A.PRED_GT, top, 0),                # nothing passes
+        (A.PRED_GT, top - 1, 0),            # only the maximum
+        (A.PRED_EQ, 0, 0),
+        (A.PRED_EQ, top, 0),
+        (A.PRED_NE, top // 3, 0),           # complement of a point
+        (A.PRED_BETWEEN, top // 4, top - top // 4),
+        (A.PRED_BETWEEN, top, top // 2),    # k0 > k1: empty range
+        (A.PRED_NOT_BETWEEN, top // 3, top // 2),
+        (A.PRED_NOT_BETWEEN, 0, top),       # nothing passes
+        (A.PRED_HALF, 0, 0),
+        (A.PRED_ALL, 0, 0),
+        (A.PRED_GE, top + 5, 0),            # bound beyond the width: nothing passes
+        (A.PRED_LT, top + 5, 0),            # bound beyond the width: everything passes
+    ]
+
+
+def _set_policy(pid):
+    from amethyst_b200 import _capi as A
+
+    t = A.Tuning(0, 0, pid, 0)
+    A.check(A.lib().amx_set_tuning(C.byref(t)))
+
+
+@pytest.fixture
+def restore_tuning():
+    yield
+    from amethyst_b200 import _capi as A
+
+    A.check(A.lib().amx_set_tuning(None))
+
+
+@pytest.mark.parametrize("bits", list(range(1, 33)))
+def test_swar_filter_and_compressstore(cuda, restore_tuning, bits):
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = [100003, 77777, 40961, 1 << 17][bits % 4]
+    v, raw = make_column(bits * 31 + 7, SLAB, bits, n)
+    col = to_gpu(raw, n, SLAB, bits)
+    for force in (1 + SWAR_BASE + bits, 0):
+        _set_policy(force)
+        for kind, k0, k1 in edge_preds(bits):
+            p = ops.predicate(kind, k0, k1, bits)
+            op = O.pred(kind, k0, k1, bits)
+            got = ops.filter(col, p).cpu().numpy().view(np.uint32)[: (n + 31) // 32]
+            assert np.array_equal(got, O.filter(raw, n, SLAB, bits, op)), ("filter", bits, kind, k0, k1)
+            out, cnt = ops.filter_compressstore(col, p, SLAB, bits)
+            want, wcnt = O.filter_compressstore(raw, n, SLAB, bits, op, SLAB, bits)
+            assert int(cnt[0].item()) == wcnt, ("count", bits, kind, k0, k1)
+            assert np.array_equal(gpu_bytes(out, wcnt), want), ("compressstore", bits, kind, k0, k1)
+
+
+@pytest.mark.parametrize("bits", [1, 3, 7, 8, 11, 13, 16, 21, 32])
+@pytest.mark.parametrize("n", [0, 1, 63, 64, 65, 4097, 32767, 32768, 32769, 262145])
+def test_swar_chain_outputs(cuda, restore_tuning, bits, n):
+    """Count, every aggregation, the mask and the compacted column in plain32 and nogaps, one
+    slab column with a predicate (policy forced), at sizes around tile edges."""
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    v, raw = make_column(bits * 7 + n, SLAB, bits, n)
+    col = to_gpu(raw, n, SLAB, bits)
+    _set_policy(1 + SWAR_BASE + bits)
+    top = (1 << bits) - 1
+    for kind, k0, k1 in [(A.PRED_LT, top // 3 + 1, 0), (A.PRED_NOT_BETWEEN, top // 5, top // 2)]:
+        p = ops.predicate(kind, k0, k1, bits)
+        op = O.pred(kind, k0, k1, bits)
+        for agg in range(6):
+            for out_fmt, out_bits in [(A.PLAIN32, 32), (A.NOGAPS, bits), (None, None)]:
+                out, mask, cnt, ag = ops.chain(col, None, A.OP_LHS, bits, p, agg, out_fmt=out_fmt,
+                                               out_bits=out_bits, want_mask=True)
+                wout, wcnt, wagg = O.chain(A.OP_LHS, (raw, SLAB, bits), None, bits, op, agg, out_fmt, out_bits, n)
+                assert int(cnt[0].item()) == wcnt
+                assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (bits, n, kind, agg)
+                gm = mask.cpu().numpy().view(np.uint32)[: (n + 31) // 32]
+                assert np.array_equal(gm, O.filter(raw, n, SLAB, bits, op))
+                if out_fmt is not None:
+                    assert np.array_equal(gpu_bytes(out, wcnt), wout), (bits, n, kind, out_fmt)
