@@ -68,6 +68,11 @@ _SIGS = {
     "amx_chain": (C.c_int, [C.POINTER(ChainDesc), _COL, _COL, _COL, _P, _P, _P, _P, C.c_size_t, _P]),
     "amx_groupby_workspace_bytes": (C.c_uint64, [C.c_uint32]),
     "amx_groupby": (C.c_int, [_COL, _COL, _P, _COL, _COL, _COL, _P, _P, C.c_size_t, _P]),
+    "amx_matmul_workspace_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32]),
+    "amx_matmul_out_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_uint32]),
+    "amx_matmul": (C.c_int, [_COL, _COL, C.c_uint32, C.c_uint32, C.c_uint32, _COL, _P, _P, C.c_size_t, _P]),
+    "amx_matmul_status": (C.c_int, [_P, _P]),
     "amx_fill_uniform": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _P]),
     "amx_fill_from_cdf": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P]),
 }

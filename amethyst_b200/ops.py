@@ -173,5 +173,29 @@ def groupby(keys: PackedColumn, vals: PackedColumn, key_fmt: int = A.PLAIN32, su
     return ok, os_, oc, ng
 
 
+def matmul_workspace(m: int, n: int, k: int, device="cuda") -> torch.Tensor:
+    """A 1024-byte-aligned workspace for amx_matmul (torch hands out 512-byte-aligned blocks)."""
+    nb = int(lib().amx_matmul_workspace_bytes(m, n, k))
+    raw = torch.empty(nb + 1024, dtype=torch.uint8, device=device)
+    off = (-raw.data_ptr()) % 1024
+    return raw[off: off + nb]
+
+
+def matmul(a: PackedColumn, b: PackedColumn, m: int, n: int, k: int, out_fmt: int = A.SLAB, out_bits: int = 0,
+           ws=None, stream=None):
+    """C = A (m x k) * B (k x n) on the integer tensor cores.  out_bits 0 picks the narrowest width
+    holding the largest entry; returns (C column, device tensor holding the width used)."""
+    dev = a.data.device
+    nb = int(lib().amx_matmul_out_bytes(out_fmt, out_bits, m, n, k, a.bits, b.bits))
+    if nb == 0 and m * n:
+        raise ValueError("unsupported matmul widths")
+    out = PackedColumn(alloc_bytes(nb, dev), m * n, out_fmt, out_bits)
+    width = torch.zeros(4, dtype=torch.int32, device=dev)
+    ws = matmul_workspace(m, n, k, dev) if ws is None else ws
+    check(lib().amx_matmul(C.byref(a.desc), C.byref(b.desc), m, n, k, C.byref(out.desc), _ptr(width), _ptr(ws),
+                           ws.numel(), _stream_ptr(stream)))
+    return out, width
+
+
 def workspace_status(ws: torch.Tensor, stream=None) -> None:
     check(lib().amx_workspace_status(_ptr(ws), _stream_ptr(stream)))

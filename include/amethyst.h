@@ -202,6 +202,27 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
                        const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
                        uint64_t* d_groups, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- matrix op ---------------------------------------------------------------------------- */
+/* C (M x N) = A (M x K) * B (K x N) over unsigned entries of at most 8 bits, exact, on the integer
+ * tensor cores (u8 x u8 -> int32).  Matrices are columns of M*K, K*N and M*N entries: AMX_SLAB
+ * matrices pad every row to whole slabs (get_matrix_element, src/common_code.cuh:124-129), the
+ * other formats are row-major.  K * (2^a_bits - 1) * (2^b_bits - 1) must stay below 2^31
+ * (AMX_ERR_UNSUPPORTED otherwise).  out->bits == 0 writes C at the narrowest width that holds
+ * its largest entry and stores that width in *d_out_bits (device memory, may be NULL); size
+ * `out` with amx_matmul_out_bytes(format, 0, ...), the widest possible case.  A nonzero
+ * out->bits masks every entry to that width.  The workspace (amx_matmul_workspace_bytes) must be
+ * 1024-byte aligned.  The reference has no matrix kernel, only the element accessors
+ * (src/common_code.cuh:65-86,118-134). */
+uint64_t amx_matmul_workspace_bytes(uint32_t M, uint32_t N, uint32_t K);
+uint64_t amx_matmul_out_bytes(uint32_t format, uint32_t out_bits, uint32_t M, uint32_t N, uint32_t K, uint32_t a_bits,
+                              uint32_t b_bits);
+amx_status amx_matmul(const amx_column* a, const amx_column* b, uint32_t M, uint32_t N, uint32_t K,
+                      const amx_column* out, uint32_t* d_out_bits, void* workspace, size_t workspace_bytes,
+                      void* stream);
+/* synchronises `stream`, then reports a device-side failure recorded by the last amx_matmul that
+ * used `workspace` (AMX_OK if none) */
+amx_status amx_matmul_status(const void* workspace, void* stream);
+
 /* ---- fused operator chain -------------------------------------------------------------- */
 /* v = op(lhs, rhs) masked to value_bits (v = lhs when rhs is NULL), keep the elements with
  * pred(v), then any of: the survivors compacted into `out`, the bitmask of pred(v) into
