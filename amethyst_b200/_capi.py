@@ -44,6 +44,15 @@ class Tuning(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+
+
+class BatchPlan(C.Structure):
+    _fields_ = [("ncols", C.c_uint32), ("threads", C.c_uint32), ("grid", C.c_uint32), ("reserved", C.c_uint32),
+                ("items", C.c_uint64), ("workspace_bytes", C.c_uint64)]
+
+
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libamethyst_b200.so")
 
 _P = C.c_void_p
@@ -73,6 +82,11 @@ _SIGS = {
                                           C.c_uint32]),
     "amx_matmul": (C.c_int, [_COL, _COL, C.c_uint32, C.c_uint32, C.c_uint32, _COL, _P, _P, C.c_size_t, _P]),
     "amx_matmul_status": (C.c_int, [_P, _P]),
+    "amx_batch_workspace_bytes": (C.c_uint64, [_COL, C.c_uint32, C.POINTER(BatchTuning)]),
+    "amx_batch_prepare": (C.c_int, [_COL, C.POINTER(Predicate), _COL, C.c_uint32, C.POINTER(BatchTuning),
+                                    C.POINTER(BatchPlan), _P, C.c_size_t, _P]),
+    "amx_batch_run": (C.c_int, [C.POINTER(BatchPlan), _P, _P, _P, C.c_size_t, _P]),
+    "amx_batch_status": (C.c_int, [_P, _P]),
     "amx_fill_uniform": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _P]),
     "amx_fill_from_cdf": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P]),
 }

@@ -1,0 +1,429 @@
+// amx_batch.cu -- filter + compressstore + sum over many slab columns of uneven length and width
+// in ONE persistent launch.
+//
+// The reference runs one launch per operator and column (src/main.cu:300-340 drives the benches
+// column by column; src/op_chaining_demo.cu:137-152 chains launches).  Here the columns of a batch
+// are cut into tiles of ~16 KB of packed input (fewer bytes for widths below 8), the tiles of all
+// columns form one work list, and persistent CTAs take work items from an atomic ticket.  Per
+// item:
+//   1. the item's column comes from a host-built item -> column map, its tile from the column's
+//      first item;
+//   2. each thread loads its slab words straight from global memory and evaluates the column's
+//      predicate field-parallel (the runtime-mask form of the single-column policy: whole-word
+//      subtractions against the column's repeated bounds);
+//   3. a block scan gives every thread its survivors' places inside the tile;
+//   4. warp 0 runs a decoupled look-back over the column's earlier items (aggregate / inclusive
+//      prefix flags in one status word per item; bounded spins) for the tile's output offset;
+//   5. survivors are gathered in shared memory and re-encoded as slabs of the column's width at
+//      that offset; the block's survivor sum goes to the column's sum with one 64-bit atomic; the
+//      column's last tile writes its count.
+// Work items are handed out in column-major order, so every item's predecessors are already
+// held by running CTAs and the look-back cannot wait on an item that has not started.
+#include <vector>
+
+#include "amx_dispatch.h"
+#include "amx_pipeline.cuh"
+
+namespace amx {
+
+struct BatchCol {
+    const unsigned long long* data;
+    unsigned long long* out;
+    uint64_t n;
+    uint64_t item0;  // first work item of the column
+    uint64_t items;  // work items of the column
+    uint64_t sw_h, sw_l1, sw_l2;
+    uint32_t bits, eps, spt, te;  // te = elements per tile = threads * spt * eps
+    uint32_t sw_mode, cv16;
+    uint64_t eps_m64;  // magic divisor of eps (udiv64)
+};
+
+struct BatchHdr {
+    unsigned long long ticket;
+    uint32_t err;
+    uint32_t pad;
+    uint64_t pad1[2];
+};
+
+constexpr uint64_t kBatchP = 1ull << 63;  // inclusive prefix published
+constexpr uint64_t kBatchA = 1ull << 62;  // tile aggregate published
+constexpr uint64_t kBatchVal = kBatchA - 1;
+constexpr uint32_t kBatchMaxSpt = 8;
+// survivors of one tile: u16 for widths <= 16 (at most 64 per thread), else u32 (at most 24 per thread)
+template <uint32_t THREADS>
+constexpr uint32_t batch_cv_bytes() { return THREADS * 128; }
+
+// slab words per thread for a width: R = spt * eps <= 64 elements, at most 8 words
+inline uint32_t batch_spt(uint32_t bits)
+{
+    const uint32_t eps = 64 / bits;
+    const uint32_t s = 64 / eps;
+    return s < 1 ? 1 : (s > kBatchMaxSpt ? kBatchMaxSpt : s);
+}
+
+__device__ __forceinline__ uint64_t batch_flags(const BatchCol& c, uint64_t x)
+{
+    const uint64_t H = c.sw_h;
+    const uint32_t mode = c.sw_mode;
+    uint64_t f = H;
+    const uint64_t xh = x | H;
+    if (mode & kSwLo) {
+        const uint64_t t = xh - c.sw_l1;
+        f = (mode & kSwLoTop) ? (x & t & H) : ((x | t) & H);
+    }
+    if (mode & kSwHi) {
+        const uint64_t t = xh - c.sw_l2;
+        const uint64_t ge = (mode & kSwHiTop) ? (x & t) : (x | t);
+        f &= ~ge;
+    }
+    if (mode & kSwNone) f = 0;
+    if (mode & kSwNeg) f ^= H;
+    return f;
+}
+
+template <uint32_t THREADS>
+__global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __restrict__ cols,
+                                                           const uint32_t* __restrict__ colmap, uint64_t total_items,
+                                                           uint64_t* status, BatchHdr* hdr,
+                                                           unsigned long long* counts, unsigned long long* sums)
+{
+    constexpr uint32_t NW = THREADS / 32;
+    extern __shared__ __align__(16) uint8_t cvbuf[];
+    __shared__ uint64_t s_item;
+    __shared__ uint32_t s_wtot[NW];
+    __shared__ unsigned long long s_wsum[NW];
+    __shared__ uint64_t s_excl;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(&hdr->ticket, 1ull);
+        __syncthreads();
+        const uint64_t item = s_item;
+        if (item >= total_items) break;
+        const uint32_t ci = __ldg(colmap + item);
+        const BatchCol c = cols[ci];
+        const uint64_t t = item - c.item0;
+        const uint64_t e0 = t * c.te;
+        const uint64_t rem = c.n - e0;
+        const uint32_t valid = rem < c.te ? (uint32_t)rem : c.te;
+        const uint32_t R = c.spt * c.eps;
+        const uint32_t B = c.bits;
+        const uint64_t FM = (1ull << B) - 1;
+
+        // 2. words and field-parallel flags
+        uint64_t x[kBatchMaxSpt], g[kBatchMaxSpt];
+        {
+            const uint64_t nslabs = (c.n + c.eps - 1) / c.eps;
+            const uint64_t s0 = t * (uint64_t)(THREADS * c.spt) + (uint64_t)tid * c.spt;
+#pragma unroll
+            for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
+                x[i] = (i < c.spt && s0 + i < nslabs) ? __ldg(c.data + s0 + i) : 0;
+            }
+            const uint32_t le0 = tid * R;
+#pragma unroll
+            for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
+                uint64_t f = i < c.spt ? batch_flags(c, x[i]) : 0;
+                const int left = (int)valid - (int)(le0 + i * c.eps);
+                f &= left <= 0 ? 0ull : (left >= (int)c.eps ? ~0ull : ((1ull << (left * B)) - 1));
+                g[i] = f;
+            }
+        }
+        uint32_t cnt = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < kBatchMaxSpt; i++) cnt += __popcll(g[i]);
+
+        // 3. block scan
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        if (lane == 31) s_wtot[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < NW; w++) {
+            const uint32_t v = s_wtot[w];
+            before += w < warp ? v : 0;
+            total += v;
+        }
+        const uint32_t pos0 = before + incl - cnt;
+
+        // 4. decoupled look-back inside the column
+        if (warp == 0) {
+            uint64_t excl = 0;
+            if (t == 0) {
+                if (lane == 0) st_relaxed_u64(&status[item], kBatchP | total);
+            }
+            else {
+                if (lane == 0) st_relaxed_u64(&status[item], kBatchA | total);
+                uint64_t j = item;  // items [c.item0, j) remain to be visited
+                bool done = false;
+                while (!done) {
+                    const bool in = j > c.item0 + lane;
+                    const uint64_t idx = j - 1 - lane;
+                    uint64_t st = in ? ld_relaxed_u64(&status[idx]) : kBatchP;
+                    uint32_t spins = 0;
+                    while (in && (st & (kBatchP | kBatchA)) == 0) {
+                        if (++spins > kWaitSpins) {
+                            record_error(&hdr->err, AMX_ERR_TIMEOUT);
+                            st = kBatchP;
+                            break;
+                        }
+                        if (spins > 8) __nanosleep(32);
+                        st = ld_relaxed_u64(&status[idx]);
+                    }
+                    const uint32_t pmask = __ballot_sync(0xffffffffu, (st & kBatchP) != 0);
+                    const uint32_t stop = pmask ? (uint32_t)(__ffs(pmask) - 1) : 31;
+                    uint64_t v = (in && lane <= stop) ? (st & kBatchVal) : 0;
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                    excl += v;
+                    done = pmask != 0;
+                    j = j > 32 ? j - 32 : 0;
+                }
+                if (lane == 0) st_relaxed_u64(&status[item], kBatchP | (excl + total));
+            }
+            if (lane == 0) s_excl = excl;
+        }
+
+        // 5. gather, sum
+        unsigned long long mysum = 0;
+        {
+            uint32_t pos = pos0;
+            const bool dense = __any_sync(0xffffffffu, 5 * cnt > 2 * R);
+#pragma unroll
+            for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
+                if (dense) {
+                    for (uint32_t k = 0; k < c.eps; k++)
+                        if ((g[i] >> (k * B + B - 1)) & 1) {
+                            const uint32_t v = (uint32_t)((x[i] >> (k * B)) & FM);
+                            if (c.cv16)
+                                reinterpret_cast<uint16_t*>(cvbuf)[pos++] = (uint16_t)v;
+                            else
+                                reinterpret_cast<uint32_t*>(cvbuf)[pos++] = v;
+                            mysum += v;
+                        }
+                }
+                else {
+                    for (uint64_t f = g[i]; f; f &= f - 1) {
+                        const int bp = __ffsll((long long)f) - 1;
+                        const uint32_t v = (uint32_t)((x[i] >> (bp - (B - 1))) & FM);
+                        if (c.cv16)
+                            reinterpret_cast<uint16_t*>(cvbuf)[pos++] = (uint16_t)v;
+                        else
+                            reinterpret_cast<uint32_t*>(cvbuf)[pos++] = v;
+                        mysum += v;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) mysum += __shfl_xor_sync(0xffffffffu, mysum, o);
+        if (lane == 0) s_wsum[warp] = mysum;
+        __syncthreads();  // survivors gathered, s_excl and the warp sums visible
+
+        const uint64_t g0 = s_excl;
+        const bool last = t + 1 == c.items;
+        OutDev o{};
+        o.data = c.out;
+        o.mask = FM;
+        o.format = AMX_SLAB;
+        o.bits = B;
+        o.eps = c.eps;
+        o.eps_m64 = c.eps_m64;
+        if (c.cv16)
+            encode_tile<uint16_t>(o, reinterpret_cast<const uint16_t*>(cvbuf), total, g0, last, tid, THREADS);
+        else
+            encode_tile<uint32_t>(o, reinterpret_cast<const uint32_t*>(cvbuf), total, g0, last, tid, THREADS);
+        if (tid == 0) {
+            unsigned long long s = 0;
+            for (uint32_t w = 0; w < NW; w++) s += s_wsum[w];
+            if (s) atomicAdd(&sums[ci], s);
+            if (last) counts[ci] = g0 + total;
+        }
+        __syncthreads();  // the buffer is free for the next item
+    }
+}
+
+}  // namespace amx
+
+using namespace amx;
+
+namespace {
+
+constexpr uint64_t kBatchHdrBytes = 256;
+
+uint64_t up256(uint64_t x) { return (x + 255) & ~255ull; }
+
+struct BatchLayout {
+    uint64_t hdr, cols, colmap, status, total;
+};
+
+BatchLayout batch_layout(uint32_t ncols, uint64_t items)
+{
+    BatchLayout l{};
+    l.hdr = 0;
+    l.cols = kBatchHdrBytes;
+    l.colmap = up256(l.cols + sizeof(BatchCol) * (uint64_t)ncols);
+    l.status = up256(l.colmap + 4 * items);
+    l.total = up256(l.status + 8 * items);
+    return l;
+}
+
+uint32_t tuned_threads(const amx_batch_tuning* t) { return (t && t->threads == 512) ? 512 : 256; }
+
+uint64_t column_items(const amx_column& c, uint32_t threads)
+{
+    const uint32_t eps = 64 / c.bits;
+    const uint64_t te = (uint64_t)threads * batch_spt(c.bits) * eps;
+    return (c.n + te - 1) / te;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t amx_batch_workspace_bytes(const amx_column* ins, uint32_t ncols, const amx_batch_tuning* tuning)
+{
+    if (!ins) return 0;
+    const uint32_t T = tuned_threads(tuning);
+    uint64_t items = 0;
+    for (uint32_t i = 0; i < ncols; i++) {
+        if (ins[i].format != AMX_SLAB || ins[i].bits < 1 || ins[i].bits > 32) return 0;
+        items += column_items(ins[i], T);
+    }
+    return batch_layout(ncols, items).total;
+}
+
+amx_status amx_batch_prepare(const amx_column* ins, const amx_predicate* preds, const amx_column* outs, uint32_t ncols,
+                             const amx_batch_tuning* tuning, amx_batch_plan* plan, void* ws, size_t ws_bytes,
+                             void* stream)
+{
+    if (!plan) return fail(AMX_ERR_INVALID_ARG, "batch_prepare: null plan");
+    if (ncols && (!ins || !preds || !outs)) return fail(AMX_ERR_INVALID_ARG, "batch_prepare: null column arrays");
+    const uint32_t T = tuned_threads(tuning);
+    std::vector<BatchCol> cols(ncols);
+    uint64_t items = 0;
+    for (uint32_t i = 0; i < ncols; i++) {
+        const amx_column& a = ins[i];
+        const amx_column& o = outs[i];
+        amx_status st = check_column(&a, "batch: input column");
+        if (st) return st;
+        if ((st = check_column(&o, "batch: output column"))) return st;
+        if (a.format != AMX_SLAB || a.bits > 32)
+            return fail(AMX_ERR_UNSUPPORTED, "batch: column %u is not a slab column of at most 32 bits", i);
+        if (o.format != AMX_SLAB || o.bits != a.bits)
+            return fail(AMX_ERR_UNSUPPORTED, "batch: output %u must be slabs of the input width", i);
+        if (o.n < a.n) return fail(AMX_ERR_INVALID_ARG, "batch: output %u capacity below input length", i);
+        PipeParams p{};
+        p.a = col_dev(&a);
+        if ((st = normalize_pred(&preds[i], p.pred_lo, p.pred_span, p.pred_neg))) return st;
+        swar_setup(p);
+        BatchCol& c = cols[i];
+        c.data = reinterpret_cast<const unsigned long long*>(a.data);
+        c.out = reinterpret_cast<unsigned long long*>(o.data);
+        c.n = a.n;
+        c.bits = a.bits;
+        c.eps = 64 / a.bits;
+        c.spt = batch_spt(a.bits);
+        c.te = T * c.spt * c.eps;
+        c.item0 = items;
+        c.items = (a.n + c.te - 1) / c.te;
+        c.sw_h = p.sw_h;
+        c.sw_l1 = p.sw_l1;
+        c.sw_l2 = p.sw_l2;
+        c.sw_mode = p.sw_mode;
+        c.cv16 = a.bits <= 16 ? 1 : 0;
+        c.eps_m64 = magic64(c.eps);
+        items += c.items;
+    }
+    const BatchLayout L = batch_layout(ncols, items);
+    if (!ws || ws_bytes < L.total)
+        return fail(AMX_ERR_WORKSPACE, "batch: workspace of %zu bytes, %llu needed", ws_bytes,
+                    (unsigned long long)L.total);
+    if (((uintptr_t)ws) & 255) return fail(AMX_ERR_ALIGNMENT, "batch: workspace not 256-byte aligned");
+    std::vector<uint32_t> colmap(items);
+    for (uint32_t i = 0; i < ncols; i++)
+        for (uint64_t k = 0; k < cols[i].items; k++) colmap[cols[i].item0 + k] = i;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    cudaError_t e = cudaSuccess;
+    if (ncols) e = cudaMemcpyAsync(w + L.cols, cols.data(), sizeof(BatchCol) * ncols, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && items)
+        e = cudaMemcpyAsync(w + L.colmap, colmap.data(), 4 * items, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host tables die with this call
+    if (e != cudaSuccess) return cuda_fail(e, "batch_prepare: table upload");
+
+    int per_sm = 0;
+    const int want = (tuning && tuning->ctas_per_sm) ? (int)tuning->ctas_per_sm : 0;
+    if (T == 512) {
+        e = cudaFuncSetAttribute(batch_fc_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_cv_bytes<512>());
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_fc_kernel<512>, 512, batch_cv_bytes<512>());
+    }
+    else {
+        e = cudaFuncSetAttribute(batch_fc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)batch_cv_bytes<256>());
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_fc_kernel<256>, 256, batch_cv_bytes<256>());
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batch_prepare: occupancy");
+    if (per_sm < 1) return fail(AMX_ERR_UNSUPPORTED, "batch: kernel does not fit on an SM");
+    if (want > 0 && want < per_sm) per_sm = want;
+    uint64_t grid = (uint64_t)per_sm * sm_count();
+    if (grid > items) grid = items ? items : 1;
+    plan->ncols = ncols;
+    plan->threads = T;
+    plan->grid = (uint32_t)grid;
+    plan->items = items;
+    plan->workspace_bytes = L.total;
+    return AMX_OK;
+}
+
+amx_status amx_batch_run(const amx_batch_plan* plan, uint64_t* d_counts, uint64_t* d_sums, void* ws, size_t ws_bytes,
+                         void* stream)
+{
+    if (!plan) return fail(AMX_ERR_INVALID_ARG, "batch_run: null plan");
+    if (plan->ncols && (!d_counts || !d_sums)) return fail(AMX_ERR_INVALID_ARG, "batch_run: null counts or sums");
+    if (!ws || ws_bytes < plan->workspace_bytes) return fail(AMX_ERR_WORKSPACE, "batch_run: workspace too small");
+    const BatchLayout L = batch_layout(plan->ncols, plan->items);
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    cudaError_t e = cudaMemsetAsync(w, 0, kBatchHdrBytes, s);
+    if (e == cudaSuccess && plan->items) e = cudaMemsetAsync(w + L.status, 0, 8 * plan->items, s);
+    if (e == cudaSuccess && plan->ncols) e = cudaMemsetAsync(d_sums, 0, 8 * (uint64_t)plan->ncols, s);
+    if (e == cudaSuccess && plan->ncols) e = cudaMemsetAsync(d_counts, 0, 8 * (uint64_t)plan->ncols, s);
+    if (e != cudaSuccess) return cuda_fail(e, "batch_run: clear");
+    if (!plan->items) return AMX_OK;
+    const BatchCol* cols = reinterpret_cast<const BatchCol*>(w + L.cols);
+    const uint32_t* colmap = reinterpret_cast<const uint32_t*>(w + L.colmap);
+    uint64_t* status = reinterpret_cast<uint64_t*>(w + L.status);
+    BatchHdr* hdr = reinterpret_cast<BatchHdr*>(w);
+    auto* cnt = reinterpret_cast<unsigned long long*>(d_counts);
+    auto* sum = reinterpret_cast<unsigned long long*>(d_sums);
+    if (plan->threads == 512)
+        batch_fc_kernel<512><<<plan->grid, 512, batch_cv_bytes<512>(), s>>>(cols, colmap, plan->items, status, hdr, cnt,
+                                                                          sum);
+    else
+        batch_fc_kernel<256><<<plan->grid, 256, batch_cv_bytes<256>(), s>>>(cols, colmap, plan->items, status, hdr, cnt,
+                                                                          sum);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "batch_run: launch");
+    return AMX_OK;
+}
+
+amx_status amx_batch_status(const void* ws, void* stream)
+{
+    if (!ws) return fail(AMX_ERR_INVALID_ARG, "batch_status: null workspace");
+    BatchHdr h{};
+    cudaError_t e = cudaMemcpyAsync(&h, ws, sizeof(h), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch_status");
+    if (h.err) return fail((amx_status)h.err, "batch: a device-side wait timed out");
+    return AMX_OK;
+}
+
+}  // extern "C"

@@ -197,5 +197,37 @@ def matmul(a: PackedColumn, b: PackedColumn, m: int, n: int, k: int, out_fmt: in
     return out, width
 
 
+class Batch:
+    """A prepared batch of slab columns for one-launch filter + compressstore + sum
+    (amx_batch_prepare / amx_batch_run).  Keeps the column arrays, outputs and workspace alive."""
+
+    def __init__(self, cols: list, preds: list, tuning: A.BatchTuning | None = None, device="cuda"):
+        self.cols = cols
+        self.outs = [PackedColumn.empty(c.n, A.SLAB, c.bits, device) for c in cols]
+        n = len(cols)
+        self.ins_arr = (A.Column * max(n, 1))(*[c.desc for c in cols])
+        self.outs_arr = (A.Column * max(n, 1))(*[o.desc for o in self.outs])
+        self.preds_arr = (A.Predicate * max(n, 1))(*preds)
+        self.tuning = tuning
+        tp = C.byref(tuning) if tuning is not None else None
+        nb = int(lib().amx_batch_workspace_bytes(self.ins_arr, n, tp))
+        self.ws = torch.empty(max(nb, 256) + 256, dtype=torch.uint8, device=device)
+        off = (-self.ws.data_ptr()) % 256
+        self.ws = self.ws[off: off + max(nb, 256)]
+        self.plan = A.BatchPlan()
+        self.counts = torch.zeros(max(n, 1), dtype=torch.int64, device=device)
+        self.sums = torch.zeros(max(n, 1), dtype=torch.int64, device=device)
+        check(lib().amx_batch_prepare(self.ins_arr, self.preds_arr, self.outs_arr, n, tp, C.byref(self.plan),
+                                      _ptr(self.ws), self.ws.numel(), _stream_ptr()))
+
+    def run(self, stream=None):
+        check(lib().amx_batch_run(C.byref(self.plan), _ptr(self.counts), _ptr(self.sums), _ptr(self.ws),
+                                  self.ws.numel(), _stream_ptr(stream)))
+        return self.counts, self.sums
+
+    def status(self, stream=None):
+        check(lib().amx_batch_status(_ptr(self.ws), _stream_ptr(stream)))
+
+
 def workspace_status(ws: torch.Tensor, stream=None) -> None:
     check(lib().amx_workspace_status(_ptr(ws), _stream_ptr(stream)))

@@ -202,6 +202,42 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
                        const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
                        uint64_t* d_groups, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- batches of columns ------------------------------------------------------------------ */
+/* Filter + compressstore + sum over `ncols` slab columns of any lengths and widths (1..32 bits)
+ * in one persistent launch.  Column i keeps the elements that pass preds[i], compacted into
+ * outs[i] (slabs of the input width, capacity >= ins[i].n); its survivor count goes to
+ * d_counts[i] and the uint64 sum of its survivors to d_sums[i].  The reference launches every
+ * operator once per column (src/main.cu:300-340).
+ *   amx_batch_prepare   validates the columns, uploads the column table to the workspace and
+ *                       fills `plan` (synchronises `stream` once; call it outside graph capture);
+ *   amx_batch_run       clears the outputs and launches the batch: stream-ordered, allocation-free
+ *                       and capturable into a CUDA graph, replayable as long as the columns and
+ *                       the workspace stay in place.
+ * Tuning (may be NULL): threads per CTA (256 or 512) and CTAs per SM (0 = as many as fit). */
+typedef struct {
+    uint32_t threads;
+    uint32_t ctas_per_sm;
+    uint32_t reserved[2];
+} amx_batch_tuning;
+
+typedef struct {
+    uint32_t ncols;
+    uint32_t threads;
+    uint32_t grid;
+    uint32_t reserved;
+    uint64_t items;
+    uint64_t workspace_bytes;
+} amx_batch_plan;
+
+uint64_t amx_batch_workspace_bytes(const amx_column* ins, uint32_t ncols, const amx_batch_tuning* tuning);
+amx_status amx_batch_prepare(const amx_column* ins, const amx_predicate* preds, const amx_column* outs, uint32_t ncols,
+                             const amx_batch_tuning* tuning, amx_batch_plan* plan, void* workspace,
+                             size_t workspace_bytes, void* stream);
+amx_status amx_batch_run(const amx_batch_plan* plan, uint64_t* d_counts, uint64_t* d_sums, void* workspace,
+                         size_t workspace_bytes, void* stream);
+/* synchronises `stream`, then reports a device-side failure recorded by the last batch run */
+amx_status amx_batch_status(const void* workspace, void* stream);
+
 /* ---- matrix op ---------------------------------------------------------------------------- */
 /* C (M x N) = A (M x K) * B (K x N) over unsigned entries of at most 8 bits, exact, on the integer
  * tensor cores (u8 x u8 -> int32).  Matrices are columns of M*K, K*N and M*N entries: AMX_SLAB
