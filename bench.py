@@ -261,6 +261,131 @@ def fc_1gib(dev, steps, warmup):
             "GB_s": byts / (ms * 1e-3) / 1e9, "ms_per_step": ms, "selectivity": c / n, "alg_bytes": byts}
 
 
+def batched_512(dev, steps):
+    """512 slab columns, lengths log-uniform in [2^12, 2^24], widths uniform in 1..32, values
+    uniform in [0, 2^w), thresholds v < T drawn for selectivity uniform in [0.01, 0.99]:
+    filter + compressstore + sum of every column in one persistent launch replayed from a CUDA
+    graph (block shape from the autotuner), against 512 sequential single-column launches."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import autotune, ops
+
+    rng = np.random.default_rng(0xBA7C4)
+    ncols = 512
+    ns = np.exp(rng.uniform(np.log(2 ** 12), np.log(2 ** 24), ncols)).astype(np.int64)
+    widths = rng.integers(1, 33, ncols)
+    sel = rng.uniform(0.01, 0.99, ncols)
+    cols, preds = [], []
+    for i in range(ncols):
+        n, w = int(ns[i]), int(widths[i])
+        cols.append(pack_gpu(n, w, 0xC010 + i, 2))
+        preds.append(ops.predicate(A.PRED_LT, max(1, int(round(sel[i] * (1 << w)))), 0, w))
+    torch.cuda.synchronize()
+    tuning, tune_times = autotune.tune_batch(cols, preds)
+    b = ops.Batch(cols, preds, tuning)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        b.run(s)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        b.run(s)
+    reps = max(3, min(steps, 20))
+    stream = torch.cuda.current_stream()
+    tot, _ = time_steps(g.replay, reps, 3, stream)
+    ms_b = tot / reps
+    counts = b.counts.cpu().numpy().view(np.uint64).copy()
+    sums = b.sums.cpu().numpy().view(np.uint64).copy()
+
+    # the same work as 512 sequential single-column launches (fused chain per column)
+    L = A.lib()
+    outs = b.outs
+    cnt = torch.zeros(2 * ncols, dtype=torch.int64, device=dev)
+    agg = torch.zeros(2 * ncols, dtype=torch.int64, device=dev)
+    ws = ops.workspace(int(ns.max()))
+    descs = [A.ChainDesc(A.OP_LHS, int(widths[i]), preds[i], A.AGG_SUM, 0) for i in range(ncols)]
+    cds = [c.desc for c in cols]
+    ods = [o.desc for o in outs]
+
+    def seq():
+        sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for i in range(ncols):
+            A.check(L.amx_chain(C.byref(descs[i]), C.byref(cds[i]), None, C.byref(ods[i]), None,
+                                C.c_void_p(cnt.data_ptr() + 16 * i), C.c_void_p(agg.data_ptr() + 16 * i),
+                                C.c_void_p(ws.data_ptr()), ws.numel(), sp))
+
+    tot2, _ = time_steps(seq, reps, 2, stream)
+    ms_s = tot2 / reps
+    sc = cnt.cpu().numpy().view(np.uint64)[0::2]
+    sa = agg.cpu().numpy().view(np.uint64)[0::2]
+    same = bool(np.array_equal(sc, counts) and np.array_equal(sa, sums))
+    in_bytes = sum(storage_bytes(2, int(widths[i]), int(ns[i])) for i in range(ncols))
+    out_bytes = sum(storage_bytes(2, int(widths[i]), int(counts[i])) for i in range(ncols))
+    byts = in_bytes + out_bytes + 16 * ncols
+    res = {"workload": "512 slab columns, n log-uniform [2^12, 2^24], widths 1..32, selectivity U[0.01, 0.99]: "
+                       "filter + compressstore + sum",
+           "elements": int(ns.sum()), "alg_bytes": byts,
+           "batched_graph": {"ms": round(ms_b, 4), "GB_s": round(byts / (ms_b * 1e-3) / 1e9, 2),
+                             "tuning": {"threads": tuning.threads, "ctas_per_sm": tuning.ctas_per_sm},
+                             "autotune_ms": {k: round(v, 4) for k, v in tune_times.items()}},
+           "sequential_512_launches": {"ms": round(ms_s, 4), "GB_s": round(byts / (ms_s * 1e-3) / 1e9, 2)},
+           "speedup": round(ms_s / ms_b, 3), "results_equal": same}
+    del g, b, cols, outs
+    torch.cuda.empty_cache()
+    return res
+
+
+def matmul_4096(dev, steps):
+    """Dense 4096 x 4096 times 4096 x 4096 over unsigned 7-bit entries in slab rows (9 per slab,
+    456 slabs per row), integer tensor cores with exact int32 accumulation, output packed at the
+    narrowest width holding the largest entry.  One step = unpack + GEMM + pack."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import datagen, ops
+
+    M = N = K = 4096
+
+    def slab_matrix(rows, cols, bits, seed):
+        eps = 64 // bits
+        rs = (cols + eps - 1) // eps
+        plain = datagen.uniform_gpu(rows * cols, bits, seed).view(rows, cols)
+        pad = torch.zeros(rows, rs * eps, dtype=torch.int32, device=dev)
+        pad[:, :cols] = plain
+        flat = ops.PackedColumn(pad.reshape(-1).contiguous().view(torch.uint8), rows * rs * eps, 0, 32)
+        col = ops.convert(flat, A.SLAB, bits)
+        return ops.PackedColumn(col.data, rows * cols, A.SLAB, bits)
+
+    a = slab_matrix(M, K, 7, 0xA11)
+    b = slab_matrix(K, N, 7, 0xB22)
+    ws = ops.matmul_workspace(M, N, K)
+    out, width = ops.matmul(a, b, M, N, K, ws=ws)
+    L = A.lib()
+
+    def step():
+        A.check(L.amx_matmul(C.byref(a.desc), C.byref(b.desc), M, N, K, C.byref(out.desc),
+                             C.c_void_p(width.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel(),
+                             C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+    reps = max(3, min(steps, 30))
+    tot, _ = time_steps(step, reps, 3, torch.cuda.current_stream())
+    ms = tot / reps
+    A.check(L.amx_matmul_status(C.c_void_p(ws.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    res = {"workload": "4096^3 u7 x u7 slab matrices -> int32 -> narrowest-width slabs",
+           "ms_per_step": round(ms, 4), "TOPS": round(2 * M * N * K / (ms * 1e-3) / 1e12, 1),
+           "out_bits": int(width[0].item())}
+    del a, b, ws, out
+    torch.cuda.empty_cache()
+    return res
+
+
 def cpu_baseline_chain(st, threads):
     """The C oracle (scalar restatement of the reference semantics) on the host cores over the
     same packed inputs: count + sum of the chain; also checks the GPU result."""
@@ -359,6 +484,14 @@ def run_gpu(args):
                 extra["fc_1gib"] = fc_1gib(dev, steps=max(3, min(args.steps, 30)), warmup=3)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["fc_1gib"] = {"error": str(e)}
+            try:
+                extra["matmul_4096"] = matmul_4096(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["matmul_4096"] = {"error": str(e)}
+            try:
+                extra["batched_512"] = batched_512(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["batched_512"] = {"error": str(e)}
             for name, kw in [("chain_50pct", {"thresh": 4160}), ("chain_plain32_in", {"a_fmt": 0, "b_fmt": 0}),
                              ("chain_plain32_out", {"out_fmt": 0})]:
                 s2, ab2, st2, ib2 = chain_workload(dev, **kw)
