@@ -87,6 +87,9 @@ _SIGS = {
                                     C.POINTER(BatchPlan), _P, C.c_size_t, _P]),
     "amx_batch_run": (C.c_int, [C.POINTER(BatchPlan), _P, _P, _P, C.c_size_t, _P]),
     "amx_batch_status": (C.c_int, [_P, _P]),
+    "amx_mlp_param_count": (C.c_uint32, [C.c_uint32]),
+    "amx_mlp_forward": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P]),
+    "amx_mlp_train_step": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, C.c_float, _P, _P]),
     "amx_fill_uniform": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _P]),
     "amx_fill_from_cdf": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P]),
 }

@@ -278,6 +278,22 @@ amx_status amx_chain(const amx_chain_desc* desc, const amx_column* lhs, const am
                      uint32_t* d_mask, uint64_t* d_count, uint64_t* d_agg, void* workspace, size_t workspace_bytes,
                      void* stream);
 
+/* ---- learned format selector ------------------------------------------------------------- */
+/* A 16 -> 64 -> 64 -> classes FP32 MLP (ReLU, softmax) that picks storage formats and widths for
+ * the intermediate columns of operator chains (amethyst_b200/selector.py builds its features and
+ * labels).  Parameters: W1[64][16] b1[64] W2[64][64] b2[64] W3[classes][64] b3[classes], as one
+ * float array of amx_mlp_param_count(classes) entries; classes 2..8.  No reference counterpart:
+ * the reference fixes every format at compile time (src/main.cu:300-340).
+ *   amx_mlp_forward     probabilities [batch][classes] for features [batch][16];
+ *   amx_mlp_train_step  one mini-batch of softmax cross-entropy and one Adam step (step >= 1;
+ *                       d_adam holds 2 * param_count floats, zero before the first step); the
+ *                       mean loss goes to *d_loss (may be NULL).  Deterministic. */
+uint32_t amx_mlp_param_count(uint32_t classes);
+amx_status amx_mlp_forward(const float* d_params, uint32_t classes, const float* d_x, uint32_t batch, float* d_probs,
+                           void* stream);
+amx_status amx_mlp_train_step(float* d_params, float* d_adam, uint32_t step, uint32_t classes, const float* d_x,
+                              const uint32_t* d_labels, uint32_t batch, float lr, float* d_loss, void* stream);
+
 /* ---- synthetic data (benchmarks and tests; no reference counterpart) --------------------- */
 /* element i = top `bits` bits of splitmix64(seed + (i+1)*0x9E3779B97F4A7C15) followed by one
  * xorshift64 (13,7,17) step, written as plain uint32 (elem_bytes 4) or uint64 (8) words */
