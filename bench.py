@@ -386,6 +386,41 @@ def matmul_4096(dev, steps):
     return res
 
 
+def groupby_2e28(dev, steps):
+    """Group-by at 1 GB: 2^28 keys Zipf(s=1.1) over 1000 groups packed at 10 bits, 2^28 values
+    uniform in [0, 2^16) packed at 16 bits; per-group uint64 sum and count."""
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import datagen, ops
+
+    n = 1 << 28
+    cdf = datagen.zipf_cdf(1000, 1.1)
+    keys32, _ = datagen.keys_from_cdf_gpu(n, cdf, 0x21F)
+    keys = ops.convert(ops.PackedColumn(keys32.view(torch.uint8), n, A.PLAIN32, 32), A.SLAB, 10)
+    del keys32
+    vals = pack_gpu(n, 16, 0x7A1, 2)
+    torch.cuda.empty_cache()
+    gws = torch.empty(int(A.lib().amx_groupby_workspace_bytes(10)) + 256, dtype=torch.uint8, device=dev)
+    gws = gws[(-gws.data_ptr()) % 256:]
+    res = {}
+
+    def step():
+        res["r"] = ops.groupby(keys, vals, ws=gws)
+
+    reps = max(3, min(steps, 20))
+    tot, _ = time_steps(step, reps, 3, torch.cuda.current_stream())
+    ms = tot / reps
+    ok, osum, ocnt, ng = res["r"]
+    byts = keys.nbytes + vals.nbytes + int(ng[0].item()) * 24
+    out = {"workload": "group-by sum+count: 2^28 Zipf(1.1) keys over 1000 groups at 10 bits, 2^28 u16 values",
+           "ms_per_step": round(ms, 4), "GB_s": round(byts / (ms * 1e-3) / 1e9, 2), "groups": int(ng[0].item()),
+           "alg_bytes": byts}
+    del keys, vals, gws, res
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_baseline_chain(st, threads):
     """The C oracle (scalar restatement of the reference semantics) on the host cores over the
     same packed inputs: count + sum of the chain; also checks the GPU result."""
@@ -484,6 +519,10 @@ def run_gpu(args):
                 extra["fc_1gib"] = fc_1gib(dev, steps=max(3, min(args.steps, 30)), warmup=3)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["fc_1gib"] = {"error": str(e)}
+            try:
+                extra["groupby_2e28"] = groupby_2e28(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["groupby_2e28"] = {"error": str(e)}
             try:
                 extra["matmul_4096"] = matmul_4096(dev, args.steps)
             except Exception as e:  # pragma: no cover - reported, not fatal
