@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
         unsigned long long mysum = 0;
         {
             uint32_t pos = pos0;
-            const bool dense = __any_sync(0xffffffffu, 5 * cnt > 2 * R);
+            const bool dense = 25 * __reduce_add_sync(0xffffffffu, cnt) > 32 * R;  // above ~4% survivors
 #pragma unroll
             for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
                 if (dense) {

@@ -305,6 +305,24 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Exclusive prefix of this warp and the tile total from the NW warp totals in wt: one shared load
+// per lane and a 4-step shuffle scan instead of every lane summing all NW entries.
+template <uint32_t NW>
+__device__ __forceinline__ void tile_prefix(volatile const uint32_t* wt, uint32_t warp, uint32_t lane,
+                                            uint32_t& before, uint32_t& total)
+{
+    static_assert(NW <= 32, "one warp total per lane");
+    uint32_t pre = lane < NW ? wt[lane] : 0;
+#pragma unroll
+    for (uint32_t o = 1; o < NW; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, pre, o);
+        if (lane >= o) pre += y;
+    }
+    total = __shfl_sync(0xffffffffu, pre, NW - 1);
+    const uint32_t b = __shfl_sync(0xffffffffu, pre, warp ? warp - 1 : 0);
+    before = warp ? b : 0;
+}
+
 // named barrier 1 over the compute warps only (the loader and look-back warps never join it)
 template <uint32_t N>
 __device__ __forceinline__ void compute_bar_n()
@@ -587,13 +605,8 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 const uint32_t incl = warp_incl_scan<uint32_t>(c);
                 if (lane == 31) wt[warp] = incl;
                 compute_bar();
-                uint32_t total = 0, before = 0;
-#pragma unroll
-                for (uint32_t w = 0; w < NW; w++) {
-                    const uint32_t xw = wt[w];
-                    before += w < warp ? xw : 0;
-                    total += xw;
-                }
+                uint32_t total, before;
+                tile_prefix<NW>(wt, warp, lane, before, total);
                 pos = before + incl - c;
                 if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
                 if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
@@ -605,7 +618,9 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 slot = cv + (size_t)q * p.slot_bytes;
             }
             if (p.has_out || p.has_agg) {
-                const bool dense = __any_sync(0xffffffffu, 5 * c > 2 * (uint32_t)R);
+                // the walk over set bits wins only below ~4% survivors in the warp
+                const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
+                const bool dense = 25 * wc > 32 * (uint32_t)R;
                 uint64_t a = 0;
                 if (p.has_out) {
                     if (cv16) {
@@ -790,12 +805,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 const uint32_t incl = warp_incl_scan<uint32_t>(c);
                 if (lane == 31) wt[warp] = incl;
                 compute_bar();
-#pragma unroll
-                for (uint32_t w = 0; w < NW; w++) {
-                    const uint32_t x = wt[w];
-                    before += w < warp ? x : 0;
-                    total += x;
-                }
+                tile_prefix<NW>(wt, warp, lane, before, total);
                 pos = before + incl - c;
             }
             uint8_t* slot = cv;

@@ -116,7 +116,8 @@ __device__ __forceinline__ void swar_flags(uint32_t mode, const uint64_t (&x)[N]
 
 // Visit the passing elements of a thread's run in element order: store each value to dst[pos++]
 // (when DST) and fold it into the aggregate `a` (when AGG).  Dense warps walk every field with a
-// predicated store; sparse warps walk the set flag bits only.
+// predicated store (no branches, independent extractions); sparse warps walk the set flag bits
+// only, a serial chain per survivor that only pays off when survivors are rare.
 template <int B, int N, typename D, bool DST, bool AGG>
 __device__ __forceinline__ void swar_visit(const uint64_t (&x)[N], const uint64_t (&g)[N], bool dense, D* dst,
                                            uint32_t pos, uint32_t agg, uint64_t& a)
