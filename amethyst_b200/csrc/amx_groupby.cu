@@ -6,14 +6,16 @@
 // narrower output column to get the reference's sums masked to the key width); counts are
 // emitted; groups come out in ascending key order (the reference's order is nondeterministic).
 //
-// 1. groupby_kernel: persistent CTAs of 512 threads walk chunks of 2^20 elements.  Lanes read
+// 1. groupby_kernel: CTAs of 512 threads walk chunks of the input.  Lanes read
 //    consecutive elements (warp-major, coalesced) straight from the packed columns and aggregate
 //    into a per-CTA shared-memory table:
 //      - keys up to 12 bits: a dense table (sum as 32-bit low word + carry word, 32-bit count);
 //      - wider keys: an open-addressing hash table of 4096 slots (claimed by atomicCAS, linear
 //        probing, 8 probes); a key that finds no slot goes straight to the global table.
-//    Each chunk ends with a flush of the shared table into a dense global table of uint64 sums
-//    and counts (2^key_bits entries) with 64-bit atomics.
+//    The CTAs are persistent (grid = CTAs that fit x SMs) and walk chunks of 2^14 elements; a CTA
+//    flushes its shared table into the dense global table of uint64 sums and counts (2^key_bits
+//    entries, 64-bit atomics) once, after its last chunk (or every 2^30 elements, before its
+//    32-bit counts could overflow).
 // 2. the groups are extracted with the tile pipeline itself: mask = filter(count != 0), then
 //    compressstore of the key indices, the sums and the counts into the caller's output columns.
 #include "amx_dispatch.h"
@@ -22,7 +24,8 @@
 namespace amx {
 
 constexpr uint32_t kGbThreads = 512;
-constexpr uint64_t kGbChunk = 1ull << 20;
+constexpr uint64_t kGbChunk = 1ull << 14;
+constexpr uint64_t kGbFlushEvery = 1ull << 30;  // elements per CTA between flushes (32-bit counts)
 constexpr uint32_t kGbDenseBits = 12;
 constexpr uint32_t kGbHashSlots = 4096;
 constexpr uint32_t kGbMaxKeyBits = 24;
@@ -77,6 +80,7 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
         tlo[i] = thi[i] = tcnt[i] = 0;
     }
     __syncthreads();
+    uint64_t seen = 0;
     for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const uint64_t e0 = chunk * kGbChunk;
         const uint64_t e1 = e0 + kGbChunk < p.n ? e0 + kGbChunk : p.n;
@@ -113,18 +117,25 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
             if (old + val < old) atomicAdd(&thi[slot], 1u);
             atomicAdd(&tcnt[slot], 1u);
         }
-        __syncthreads();
-        for (uint32_t i = tid; i < slots; i += blockDim.x) {
-            const uint32_t c = tcnt[i];
-            if (c) {
-                const uint32_t key = p.dense ? i : tkey[i];
-                atomicAdd(&p.gsum[key], ((unsigned long long)thi[i] << 32) | tlo[i]);
-                atomicAdd(&p.gcnt[key], (unsigned long long)c);
+        // the shared table only goes to the global table when this CTA is done, or before its
+        // 32-bit counts could overflow
+        seen += e1 - e0;
+        const bool last = chunk + gridDim.x >= nchunks;
+        if (last || seen >= kGbFlushEvery) {
+            __syncthreads();
+            for (uint32_t i = tid; i < slots; i += blockDim.x) {
+                const uint32_t c = tcnt[i];
+                if (c) {
+                    const uint32_t key = p.dense ? i : tkey[i];
+                    atomicAdd(&p.gsum[key], ((unsigned long long)thi[i] << 32) | tlo[i]);
+                    atomicAdd(&p.gcnt[key], (unsigned long long)c);
+                }
+                tkey[i] = kEmptyKey;
+                tlo[i] = thi[i] = tcnt[i] = 0;
             }
-            tkey[i] = kEmptyKey;
-            tlo[i] = thi[i] = tcnt[i] = 0;
+            __syncthreads();
+            seen = 0;
         }
-        __syncthreads();
     }
 }
 
