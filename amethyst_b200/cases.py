@@ -1,0 +1,146 @@
+"""Named single-GPU workloads of the operator layer, for timing and profiling one kernel at a time.
+
+    python -m amethyst_b200.cases <case> [reps]
+
+prints one JSON line with the mean milliseconds per call (CUDA events, after 3 warm-up calls) and
+packed GB/s (or TOPS for the matrix multiply).  Inputs are generated on the GPU (seeded) and are
+larger than the 126 MB L2 unless the case says otherwise.
+
+  chain      A 2^26 x u7 slabs + B 2^26 x u13 slabs -> C at 14 bits, keep C >= 2^13, compressstore
+             to 14-bit slabs, sum (one amx_chain call)
+  fcB        filter v < 205 * 2^(B-11) + compressstore over 2^24 slabs of width B (e.g. fc11)
+  filterB    filter -> bitmask over 2^24 slabs of width B
+  matmul     4096^3 u7 x u7 slab matrices -> narrowest-width slabs (unpack + GEMM + pack)
+  batch64    64 slab columns, lengths log-uniform in [2^16, 2^22], widths 1..32: one batch run
+  groupby    2^26 Zipf(1.1) keys over 1000 groups at 10 bits, 2^26 u16 values at 16 bits
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import sys
+
+import numpy as np
+import torch
+
+from . import _capi as A
+from . import datagen, ops
+
+
+def _gen(n, bits, seed, fmt=A.SLAB):
+    plain = datagen.uniform_gpu(n, bits, seed)
+    return ops.convert(ops.PackedColumn(plain.view(torch.uint8), n, A.PLAIN32, 32), fmt, bits)
+
+
+def _time(fn, reps):
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def case(name: str, reps: int = 10) -> dict:
+    L = A.lib()
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if name == "chain":
+        n = 1 << 26
+        a, b = _gen(n, 7, 0x5EEDA), _gen(n, 13, 0x5EEDB)
+        out = ops.PackedColumn.empty(n, A.SLAB, 14)
+        cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+        agg = torch.zeros(2, dtype=torch.int64, device="cuda")
+        ws = ops.workspace(n)
+        desc = A.ChainDesc(A.OP_ADD, 14, ops.predicate(A.PRED_GE, 1 << 13, 0, 14), A.AGG_SUM, 0)
+        ad, bd, od = a.desc, b.desc, out.desc
+
+        def step():
+            A.check(L.amx_chain(C.byref(desc), C.byref(ad), C.byref(bd), C.byref(od), None,
+                                C.c_void_p(cnt.data_ptr()), C.c_void_p(agg.data_ptr()), C.c_void_p(ws.data_ptr()),
+                                ws.numel(), s))
+
+        ms = _time(step, reps)
+        byts = a.nbytes + b.nbytes + ops.storage_bytes(A.SLAB, 14, int(cnt[0].item())) + 16
+        return {"case": name, "ms": ms, "GB_s": byts / ms / 1e6}
+    if name.startswith("fc") or name.startswith("filter"):
+        flt = name.startswith("filter")
+        bits = int(name[6:] if flt else name[2:])
+        n = (1 << 24) * (64 // bits)
+        col = _gen(n, bits, 0xC0FFEE)
+        ws = ops.workspace(n)
+        thr = (205 << (bits - 11)) if bits >= 11 else max(1, 205 >> (11 - bits))
+        pred = ops.predicate(A.PRED_LT, thr, 0, bits)
+        cd = col.desc
+        if flt:
+            mask = torch.zeros(n // 32 + 64, dtype=torch.int32, device="cuda")
+
+            def step():
+                A.check(L.amx_filter(C.byref(cd), C.byref(pred), C.c_void_p(mask.data_ptr()),
+                                     C.c_void_p(ws.data_ptr()), ws.numel(), s))
+
+            ms = _time(step, reps)
+            return {"case": name, "ms": ms, "GB_s": (col.nbytes + n // 8) / ms / 1e6}
+        out = ops.PackedColumn.empty(n, A.SLAB, bits)
+        cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+        od = out.desc
+
+        def step():
+            A.check(L.amx_filter_compressstore(C.byref(cd), C.byref(pred), C.byref(od), C.c_void_p(cnt.data_ptr()),
+                                               C.c_void_p(ws.data_ptr()), ws.numel(), s))
+
+        ms = _time(step, reps)
+        byts = col.nbytes + ops.storage_bytes(A.SLAB, bits, int(cnt[0].item())) + 8
+        return {"case": name, "ms": ms, "GB_s": byts / ms / 1e6}
+    if name == "matmul":
+        M = N = K = 4096
+
+        def slab_matrix(rows, cols, bits, seed):
+            eps = 64 // bits
+            rs = (cols + eps - 1) // eps
+            plain = datagen.uniform_gpu(rows * cols, bits, seed).view(rows, cols)
+            pad = torch.zeros(rows, rs * eps, dtype=torch.int32, device="cuda")
+            pad[:, :cols] = plain
+            flat = ops.PackedColumn(pad.reshape(-1).contiguous().view(torch.uint8), rows * rs * eps, A.PLAIN32, 32)
+            c = ops.convert(flat, A.SLAB, bits)
+            return ops.PackedColumn(c.data, rows * cols, A.SLAB, bits)
+
+        a, b = slab_matrix(M, K, 7, 0xA11), slab_matrix(K, N, 7, 0xB22)
+        ws = ops.matmul_workspace(M, N, K)
+        out, width = ops.matmul(a, b, M, N, K, ws=ws)
+
+        def step():
+            A.check(L.amx_matmul(C.byref(a.desc), C.byref(b.desc), M, N, K, C.byref(out.desc),
+                                 C.c_void_p(width.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel(), s))
+
+        ms = _time(step, reps)
+        return {"case": name, "ms": ms, "TOPS": 2 * M * N * K / ms / 1e9, "out_bits": int(width[0].item())}
+    if name == "batch64":
+        rng = np.random.default_rng(5)
+        cols, preds = [], []
+        for i in range(64):
+            n = int(np.exp(rng.uniform(np.log(2 ** 16), np.log(2 ** 22))))
+            w = int(rng.integers(1, 33))
+            cols.append(_gen(n, w, 77 + i))
+            preds.append(ops.predicate(A.PRED_LT, max(1, int(rng.uniform(0.01, 0.99) * (1 << w))), 0, w))
+        b = ops.Batch(cols, preds, A.BatchTuning(512, 2))
+        ms = _time(b.run, reps)
+        tot = sum(ops.storage_bytes(A.SLAB, c.bits, c.n) for c in cols)
+        return {"case": name, "ms": ms, "GB_s": tot / ms / 1e6}
+    if name == "groupby":
+        n = 1 << 26
+        k32, _ = datagen.keys_from_cdf_gpu(n, datagen.zipf_cdf(1000, 1.1), 3)
+        keys = ops.convert(ops.PackedColumn(k32.view(torch.uint8), n, A.PLAIN32, 32), A.SLAB, 10)
+        vals = _gen(n, 16, 4)
+        gws = torch.empty(int(L.amx_groupby_workspace_bytes(10)) + 256, dtype=torch.uint8, device="cuda")
+        gws = gws[(-gws.data_ptr()) % 256:]
+        ms = _time(lambda: ops.groupby(keys, vals, ws=gws), reps)
+        return {"case": name, "ms": ms, "GB_s": (keys.nbytes + vals.nbytes) / ms / 1e6}
+    raise ValueError(f"unknown case {name}")
+
+
+if __name__ == "__main__":
+    print(json.dumps(case(sys.argv[1], int(sys.argv[2]) if len(sys.argv) > 2 else 10)))
