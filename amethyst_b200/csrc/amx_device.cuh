@@ -53,14 +53,30 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
-// Bounded wait on an mbarrier phase.  Returns false when the limit ran out; the caller
-// records AMX_ERR_TIMEOUT and stops using the stage.
+// try_wait that suspends the thread until the phase completes or `ns` nanoseconds pass, so a
+// waiting warp issues a handful of instructions per wait instead of a spin loop
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase: at most kWaitSuspends suspensions of kWaitSuspendNs each
+// (about 1.3 s in all).  Returns false when the limit ran out; the caller records
+// AMX_ERR_TIMEOUT and stops using the stage.
+constexpr uint32_t kWaitSuspendNs = 20000;
+constexpr uint32_t kWaitSuspends = 1u << 16;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
 {
-    for (uint32_t i = 0; i < kWaitSpins; i++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (i > 64) __nanosleep(64);
-    }
+    for (uint32_t i = 0; i < kWaitSuspends; i++)
+        if (mbar_try_wait_hint(bar, parity, kWaitSuspendNs)) return true;
     return false;
 }
 
