@@ -386,6 +386,54 @@ def matmul_4096(dev, steps):
     return res
 
 
+def fc_cfg1(dev, steps):
+    """The plain filter+compressstore configuration: 2^24 uint32 values uniform in [0, 2^11) in
+    11-bit slabs (26.8 MB, smaller than L2), predicate v < 205, output in 11-bit slabs.  L2 is
+    flushed (a 256 MB buffer rewritten) before every timed call, outside its event pair."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = 1 << 24
+    col = pack_gpu(n, 11, 0xC0FFEE, 2)
+    out = ops.PackedColumn.empty(n, 2, 11)
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    ws = ops.workspace(n)
+    pred = ops.predicate(A.PRED_LT, 205, 0, 11)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    L = A.lib()
+    cd, od = col.desc, out.desc
+    stream = torch.cuda.current_stream()
+
+    def step():
+        A.check(L.amx_filter_compressstore(C.byref(cd), C.byref(pred), C.byref(od), C.c_void_p(cnt.data_ptr()),
+                                           C.c_void_p(ws.data_ptr()), ws.numel(), C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(3):
+        step()
+    reps = max(3, min(steps, 30))
+    ms = 0.0
+    for _ in range(reps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= reps
+    c = int(cnt[0].item())
+    byts = storage_bytes(2, 11, n) + storage_bytes(2, 11, c) + 8
+    del col, out, ws, flush
+    torch.cuda.empty_cache()
+    return {"workload": "filter v<205 + compressstore, 2^24 elements in 11-bit slabs (26.8 MB), L2 flushed per call",
+            "GB_s": round(byts / (ms * 1e-3) / 1e9, 2), "ms_per_step": round(ms, 5), "selectivity": c / n,
+            "alg_bytes": byts}
+
+
 def groupby_2e28(dev, steps):
     """Group-by at 1 GB: 2^28 keys Zipf(s=1.1) over 1000 groups packed at 10 bits, 2^28 values
     uniform in [0, 2^16) packed at 16 bits; per-group uint64 sum and count."""
@@ -519,6 +567,10 @@ def run_gpu(args):
                 extra["fc_1gib"] = fc_1gib(dev, steps=max(3, min(args.steps, 30)), warmup=3)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["fc_1gib"] = {"error": str(e)}
+            try:
+                extra["fc_cfg1"] = fc_cfg1(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["fc_cfg1"] = {"error": str(e)}
             try:
                 extra["groupby_2e28"] = groupby_2e28(dev, args.steps)
             except Exception as e:  # pragma: no cover - reported, not fatal
