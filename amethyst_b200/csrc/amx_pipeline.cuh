@@ -1,18 +1,21 @@
 // amx_pipeline.cuh -- the tile pipeline kernel behind filter, compressstore, binary ops,
 // conversion, aggregation and fused chains.
 //
-// Persistent CTAs (one per SM) with three warp roles, handing work over through shared-memory
-// mbarriers so that no compute warp ever waits on global-memory latency:
+// Persistent CTAs (one per SM) with four warp roles, handing work over through shared-memory
+// mbarriers so that no compute warp waits on global-memory latency:
 //   * the loader warp (one lane) takes tiles from an atomic ticket counter and stages each
 //     tile's bytes of every input into a ring of 2..8 shared-memory stages with 1-D bulk
 //     copies (cp.async.bulk, completion on the stage's `full` mbarrier);
-//   * 8 or 16 compute warps decode R elements per thread straight from the staged packed words
-//     (a policy: warp-major runtime-width readers or thread-contiguous compile-time-width
-//     readers), apply the op and the predicate, build the bitmask / aggregate / count, scan the
-//     tile's survivors, publish the count for the decoupled look-back, gather the survivors in
-//     shared memory, and re-encode the PREVIOUS tile's survivors in the output format;
-//   * the look-back warp turns each tile's published count into its output offset (the tile's
-//     predecessors have had a whole tile of time to publish) and hands it to the compute warps.
+//   * 16 compute warps decode R elements per thread straight from the staged packed words (a
+//     policy: field-parallel slab words, thread-contiguous compile-time-width readers, or
+//     warp-major runtime-width readers), apply the op and the predicate, build the bitmask /
+//     aggregate / count, scan the tile's survivors, publish the count for the look-back, and
+//     gather the survivors into one of up to four shared-memory slots;
+//   * the look-back warp turns each tile's published count into its output offset: the CTA's
+//     tiles arrive in ticket order, so the offset is the end of the CTA's previous tile plus the
+//     counts of the tiles other CTAs took in between;
+//   * four encoder warps re-encode each slot's survivors in the output format at that offset and
+//     hand the slot back to the compute warps.
 // Replaces the reference's separate filter / popcount / CUB scan / write kernels
 // (src/kernels/filter_slabs.cuh:4-57, src/kernels/compressstore_slabs.cuh:4-206,
 // src/benchs/bench_compressstore_slabs.cu:38-56) with one pass and no mask round trip.
