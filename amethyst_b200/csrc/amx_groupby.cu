@@ -6,16 +6,15 @@
 // narrower output column to get the reference's sums masked to the key width); counts are
 // emitted; groups come out in ascending key order (the reference's order is nondeterministic).
 //
-// 1. groupby_kernel: CTAs of 512 threads walk chunks of the input.  Lanes read
-//    consecutive elements (warp-major, coalesced) straight from the packed columns and aggregate
-//    into a per-CTA shared-memory table:
+// 1. groupby_kernel: persistent CTAs of 512 threads (grid = CTAs that fit x SMs) walk chunks of
+//    2^14 elements.  Each thread reads a run of 32 consecutive elements of the chunk straight from
+//    the packed columns, one storage word at a time, and aggregates into a per-CTA shared table:
 //      - keys up to 12 bits: a dense table (sum as 32-bit low word + carry word, 32-bit count);
 //      - wider keys: an open-addressing hash table of 4096 slots (claimed by atomicCAS, linear
 //        probing, 8 probes); a key that finds no slot goes straight to the global table.
-//    The CTAs are persistent (grid = CTAs that fit x SMs) and walk chunks of 2^14 elements; a CTA
-//    flushes its shared table into the dense global table of uint64 sums and counts (2^key_bits
-//    entries, 64-bit atomics) once, after its last chunk (or every 2^30 elements, before its
-//    32-bit counts could overflow).
+//    A CTA flushes its shared table into the dense global table of uint64 sums and counts
+//    (2^key_bits entries, 64-bit atomics) once, after its last chunk (or every 2^30 elements,
+//    before its 32-bit counts could overflow).
 // 2. the groups are extracted with the tile pipeline itself: mask = filter(count != 0), then
 //    compressstore of the key indices, the sums and the counts into the caller's output columns.
 #include "amx_dispatch.h"
@@ -25,6 +24,8 @@ namespace amx {
 
 constexpr uint32_t kGbThreads = 512;
 constexpr uint64_t kGbChunk = 1ull << 14;
+constexpr uint32_t kGbRun = 32;  // consecutive elements per thread
+static_assert(kGbThreads * kGbRun == kGbChunk, "a chunk is one run per thread");
 constexpr uint64_t kGbFlushEvery = 1ull << 30;  // elements per CTA between flushes (32-bit counts)
 constexpr uint32_t kGbDenseBits = 12;
 constexpr uint32_t kGbHashSlots = 4096;
@@ -64,6 +65,60 @@ __device__ __forceinline__ uint64_t load_elem(const ColDev& c, uint64_t e)
     }
 }
 
+// Consecutive elements e, e + 1, ... of a column: one load per storage word instead of one per
+// element, and one division by the slab's field count per run instead of one per element.
+struct SeqReader {
+    const unsigned long long* w;
+    uint64_t cur;     // slab / nogaps: current word
+    uint64_t wi;      // index of the current word
+    uint64_t bitpos;  // nogaps: bit of the next element
+    uint32_t k;       // slab: field of the next element in `cur`
+};
+
+__device__ __forceinline__ SeqReader seq_open(const ColDev& c, uint64_t e)
+{
+    SeqReader r{};
+    r.w = reinterpret_cast<const unsigned long long*>(c.data);
+    switch (c.format) {
+        case AMX_PLAIN32:
+        case AMX_PLAIN64: r.wi = e; break;
+        case AMX_SLAB: {
+            r.wi = udiv64(e, c.magic64, c.eps);
+            r.k = (uint32_t)(e - r.wi * c.eps);
+            r.cur = __ldg(r.w + r.wi);
+            break;
+        }
+        default: r.bitpos = e * c.bits; break;
+    }
+    return r;
+}
+
+// the next element; `more` says whether another element of this run follows
+__device__ __forceinline__ uint64_t seq_next(const ColDev& c, SeqReader& r, bool more)
+{
+    switch (c.format) {
+        case AMX_PLAIN32: return __ldg(reinterpret_cast<const uint32_t*>(c.data) + r.wi++) & c.mask;
+        case AMX_PLAIN64: return __ldg(r.w + r.wi++) & c.mask;
+        case AMX_SLAB: {
+            const uint64_t v = (r.cur >> (r.k * c.bits)) & c.mask;
+            if (++r.k == c.eps) {
+                r.k = 0;
+                ++r.wi;
+                if (more) r.cur = __ldg(r.w + r.wi);
+            }
+            return v;
+        }
+        default: {
+            const uint64_t wi = r.bitpos >> 6;
+            const uint32_t off = (uint32_t)(r.bitpos & 63);
+            uint64_t x = __ldg(r.w + wi) >> off;
+            if (off + c.bits > 64) x |= (uint64_t)__ldg(r.w + wi + 1) << (64 - off);
+            r.bitpos += c.bits;
+            return x & c.mask;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_constant__ GbParams p)
 {
     extern __shared__ __align__(16) uint32_t tab[];
@@ -84,10 +139,19 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
     for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const uint64_t e0 = chunk * kGbChunk;
         const uint64_t e1 = e0 + kGbChunk < p.n ? e0 + kGbChunk : p.n;
-        for (uint64_t e = e0 + tid; e < e1; e += blockDim.x) {
+        // each thread walks a run of kGbRun consecutive elements of the chunk
+        const uint64_t r0 = e0 + (uint64_t)tid * kGbRun;
+        const uint32_t rn = r0 >= e1 ? 0 : (uint32_t)(e1 - r0 < kGbRun ? e1 - r0 : kGbRun);
+        SeqReader kr{}, vr{};
+        if (rn) {
+            kr = seq_open(p.k, r0);
+            vr = seq_open(p.v, r0);
+        }
+        for (uint32_t i = 0; i < rn; i++) {
+            const uint64_t e = r0 + i;
+            const uint32_t key = (uint32_t)seq_next(p.k, kr, i + 1 < rn);
+            const uint32_t val = (uint32_t)seq_next(p.v, vr, i + 1 < rn);
             if (p.mask && !((__ldg(p.mask + (e >> 5)) >> (e & 31)) & 1u)) continue;
-            const uint32_t key = (uint32_t)load_elem(p.k, e);
-            const uint32_t val = (uint32_t)load_elem(p.v, e);
             uint32_t slot = key;
             if (!p.dense) {
                 uint32_t h = (key * 2654435761u) >> 20;  // 12 bits: 4096 slots
