@@ -41,7 +41,7 @@ class ChainDesc(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("staged_bytes", C.c_uint32), ("compact_stages", C.c_uint32), ("policy", C.c_int32),
-                ("reserved", C.c_uint32)]
+                ("max_ctas", C.c_uint32)]
 
 
 class BatchTuning(C.Structure):

@@ -10,11 +10,12 @@
 //    2^14 elements.  Each thread reads a run of 32 consecutive elements of the chunk straight from
 //    the packed columns, one storage word at a time, and aggregates into a per-CTA shared table:
 //      - keys up to 12 bits: a dense table (sum as 32-bit low word + carry word, 32-bit count);
+//        values of at most 18 bits need no carry word (the table is flushed before a sum wraps);
 //      - wider keys: an open-addressing hash table of 4096 slots (claimed by atomicCAS, linear
 //        probing, 8 probes); a key that finds no slot goes straight to the global table.
 //    A CTA flushes its shared table into the dense global table of uint64 sums and counts
-//    (2^key_bits entries, 64-bit atomics) once, after its last chunk (or every 2^30 elements,
-//    before its 32-bit counts could overflow).
+//    (2^key_bits entries, 64-bit atomics) once, after its last chunk, or every 2^(32 - value
+//    bits) elements (carry-free sums, at most 2^30) before a 32-bit field could overflow.
 // 2. the groups are extracted with the tile pipeline itself: mask = filter(count != 0), then
 //    compressstore of the key indices, the sums and the counts into the caller's output columns.
 #include "amx_dispatch.h"
@@ -38,6 +39,7 @@ struct GbParams {
     uint64_t n;
     uint32_t kbits;
     uint32_t dense;
+    uint64_t flush_every;  // elements per CTA between flushes of its shared table
     unsigned long long* gsum;
     unsigned long long* gcnt;
 };
@@ -119,82 +121,157 @@ __device__ __forceinline__ uint64_t seq_next(const ColDev& c, SeqReader& r, bool
     }
 }
 
+// Slab column read as a run of consecutive elements: the current word is shifted down by one
+// field per element, so an element costs a mask, a shift and a field-count test.
+struct SlabRun {
+    const unsigned long long* w;
+    uint64_t cur;  // current word, shifted so that the next element sits in the low bits
+    uint64_t wi;
+    uint32_t k;    // field of the next element
+};
+
+__device__ __forceinline__ SlabRun slab_open(const ColDev& c, uint64_t e)
+{
+    SlabRun r;
+    r.w = reinterpret_cast<const unsigned long long*>(c.data);
+    r.wi = udiv64(e, c.magic64, c.eps);
+    r.k = (uint32_t)(e - r.wi * c.eps);
+    r.cur = __ldg(r.w + r.wi) >> (r.k * c.bits);
+    return r;
+}
+
+__device__ __forceinline__ uint32_t slab_next(const ColDev& c, SlabRun& r, bool more)
+{
+    const uint32_t v = (uint32_t)r.cur & (uint32_t)c.mask;
+    r.cur >>= c.bits;
+    if (++r.k == c.eps) {
+        r.k = 0;
+        ++r.wi;
+        if (more) r.cur = __ldg(r.w + r.wi);
+    }
+    return v;
+}
+
+// A run reader: the slab form above when the column's format is known to be AMX_SLAB at
+// compile time, else the general SeqReader (any format, chosen at run time).
+template <bool SLAB>
+struct RunReader {
+    SeqReader r;
+    __device__ __forceinline__ void open(const ColDev& c, uint64_t e) { r = seq_open(c, e); }
+    __device__ __forceinline__ uint32_t next(const ColDev& c, bool more) { return (uint32_t)seq_next(c, r, more); }
+};
+template <>
+struct RunReader<true> {
+    SlabRun r;
+    __device__ __forceinline__ void open(const ColDev& c, uint64_t e) { r = slab_open(c, e); }
+    __device__ __forceinline__ uint32_t next(const ColDev& c, bool more) { return slab_next(c, r, more); }
+};
+
+// Narrow values (at most kGbNoCarryBits bits) need no carry word: the CTA flushes its table
+// every gb_flush_every(value bits) elements, few enough that a 32-bit sum cannot wrap, so an
+// element is two 32-bit shared-memory adds whose results are not read back.
+constexpr uint32_t kGbNoCarryBits = 18;
+
+__host__ __device__ constexpr uint64_t gb_flush_every(uint32_t vbits)
+{
+    // sums <= flush * (2^vbits - 1) < 2^32; counts <= flush <= 2^30; whole chunks
+    return vbits > kGbNoCarryBits || 32 - vbits >= 30 ? kGbFlushEvery : (1ull << (32 - vbits));
+}
+static_assert(gb_flush_every(kGbNoCarryBits) % kGbChunk == 0, "flushes fall on chunk boundaries");
+
+// Hash table probe: the slot holding `key`, claiming an empty one if needed; kEmptyKey when
+// 8 probes find neither.
+__device__ __forceinline__ uint32_t gb_probe(uint32_t* tkey, uint32_t key)
+{
+    const uint32_t h = (key * 2654435761u) >> 20;  // 12 bits: 4096 slots
+    for (int probe = 0; probe < 8; probe++) {
+        const uint32_t sl = (h + probe) & (kGbHashSlots - 1);
+        const uint32_t cur = tkey[sl];
+        if (cur == key) return sl;
+        if (cur == kEmptyKey) {
+            const uint32_t prev = atomicCAS(&tkey[sl], kEmptyKey, key);
+            if (prev == kEmptyKey || prev == key) return sl;
+        }
+    }
+    return kEmptyKey;
+}
+
+template <bool KSLAB, bool VSLAB, bool DENSE, bool NOCARRY>
 __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_constant__ GbParams p)
 {
     extern __shared__ __align__(16) uint32_t tab[];
-    const uint32_t slots = p.dense ? (1u << p.kbits) : kGbHashSlots;
-    uint32_t* tkey = tab;                 // hash: key per slot
-    uint32_t* tlo = tab + slots;          // low 32 bits of the sum
-    uint32_t* thi = tab + 2 * slots;      // carries out of the low word
-    uint32_t* tcnt = tab + 3 * slots;     // count
+    const uint32_t slots = DENSE ? (1u << p.kbits) : kGbHashSlots;
+    uint32_t* tkey = tab;              // hash: key per slot
+    uint32_t* tlo = tab + slots;       // sum (low 32 bits)
+    uint32_t* thi = tab + 2 * slots;   // carries out of the low word (unused when NOCARRY)
+    uint32_t* tcnt = tab + 3 * slots;  // count
     const uint32_t tid = threadIdx.x;
     const uint64_t nchunks = (p.n + kGbChunk - 1) / kGbChunk;
+    const uint64_t flush_every = p.flush_every;
 
-    for (uint32_t i = tid; i < slots; i += blockDim.x) {
-        tkey[i] = kEmptyKey;
-        tlo[i] = thi[i] = tcnt[i] = 0;
-    }
+    auto clear = [&]() {
+        for (uint32_t i = tid; i < slots; i += blockDim.x) {
+            if (!DENSE) tkey[i] = kEmptyKey;
+            tlo[i] = thi[i] = tcnt[i] = 0;
+        }
+    };
+    clear();
     __syncthreads();
     uint64_t seen = 0;
     for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const uint64_t e0 = chunk * kGbChunk;
         const uint64_t e1 = e0 + kGbChunk < p.n ? e0 + kGbChunk : p.n;
-        // each thread walks a run of kGbRun consecutive elements of the chunk
+        // each thread walks a run of kGbRun consecutive elements of the chunk; a run starts on
+        // a multiple of 32, so its mask bits are one mask word
         const uint64_t r0 = e0 + (uint64_t)tid * kGbRun;
         const uint32_t rn = r0 >= e1 ? 0 : (uint32_t)(e1 - r0 < kGbRun ? e1 - r0 : kGbRun);
-        SeqReader kr{}, vr{};
         if (rn) {
-            kr = seq_open(p.k, r0);
-            vr = seq_open(p.v, r0);
-        }
-        for (uint32_t i = 0; i < rn; i++) {
-            const uint64_t e = r0 + i;
-            const uint32_t key = (uint32_t)seq_next(p.k, kr, i + 1 < rn);
-            const uint32_t val = (uint32_t)seq_next(p.v, vr, i + 1 < rn);
-            if (p.mask && !((__ldg(p.mask + (e >> 5)) >> (e & 31)) & 1u)) continue;
-            uint32_t slot = key;
-            if (!p.dense) {
-                uint32_t h = (key * 2654435761u) >> 20;  // 12 bits: 4096 slots
-                slot = kEmptyKey;
-                for (int probe = 0; probe < 8; probe++) {
-                    const uint32_t sl = (h + probe) & (kGbHashSlots - 1);
-                    const uint32_t cur = tkey[sl];
-                    if (cur == key) {
-                        slot = sl;
-                        break;
-                    }
-                    if (cur == kEmptyKey) {
-                        const uint32_t prev = atomicCAS(&tkey[sl], kEmptyKey, key);
-                        if (prev == kEmptyKey || prev == key) {
-                            slot = sl;
-                            break;
-                        }
+            RunReader<KSLAB> kr;
+            RunReader<VSLAB> vr;
+            kr.open(p.k, r0);
+            vr.open(p.v, r0);
+            const uint32_t mw = p.mask ? __ldg(p.mask + (r0 >> 5)) : 0xffffffffu;
+#pragma unroll 4
+            for (uint32_t i = 0; i < rn; i++) {
+                const bool more = i + 1 < rn;
+                const uint32_t key = kr.next(p.k, more);
+                const uint32_t val = vr.next(p.v, more);
+                if (!((mw >> i) & 1u)) continue;
+                uint32_t slot = key;
+                if (!DENSE) {
+                    slot = gb_probe(tkey, key);
+                    if (slot == kEmptyKey) {  // table crowded: spill to the global table
+                        atomicAdd(&p.gsum[key], (unsigned long long)val);
+                        atomicAdd(&p.gcnt[key], 1ull);
+                        continue;
                     }
                 }
-                if (slot == kEmptyKey) {  // table crowded: spill to the global table
-                    atomicAdd(&p.gsum[key], (unsigned long long)val);
-                    atomicAdd(&p.gcnt[key], 1ull);
-                    continue;
+                if (NOCARRY) {
+                    atomicAdd(&tlo[slot], val);
+                    atomicAdd(&tcnt[slot], 1u);
+                }
+                else {
+                    const uint32_t old = atomicAdd(&tlo[slot], val);
+                    if (old + val < old) atomicAdd(&thi[slot], 1u);
+                    atomicAdd(&tcnt[slot], 1u);
                 }
             }
-            const uint32_t old = atomicAdd(&tlo[slot], val);
-            if (old + val < old) atomicAdd(&thi[slot], 1u);
-            atomicAdd(&tcnt[slot], 1u);
         }
         // the shared table only goes to the global table when this CTA is done, or before its
-        // 32-bit counts could overflow
+        // fields could overflow
         seen += e1 - e0;
         const bool last = chunk + gridDim.x >= nchunks;
-        if (last || seen >= kGbFlushEvery) {
+        if (last || seen >= flush_every) {
             __syncthreads();
             for (uint32_t i = tid; i < slots; i += blockDim.x) {
                 const uint32_t c = tcnt[i];
+                const uint64_t sum = NOCARRY ? tlo[i] : ((uint64_t)thi[i] << 32) | tlo[i];
                 if (c) {
-                    const uint32_t key = p.dense ? i : tkey[i];
-                    atomicAdd(&p.gsum[key], ((unsigned long long)thi[i] << 32) | tlo[i]);
+                    const uint32_t key = DENSE ? i : tkey[i];
+                    atomicAdd(&p.gsum[key], (unsigned long long)sum);
                     atomicAdd(&p.gcnt[key], (unsigned long long)c);
                 }
-                tkey[i] = kEmptyKey;
+                if (!DENSE) tkey[i] = kEmptyKey;  // each thread clears the slots it flushed
                 tlo[i] = thi[i] = tcnt[i] = 0;
             }
             __syncthreads();
@@ -219,6 +296,19 @@ __global__ void iota_kernel(uint32_t* out, uint64_t n)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)i;
+}
+
+// the aggregation kernel for a key / value format pair, table kind and carry handling
+static const void* gb_kernel(bool kslab, bool vslab, bool dense, bool nocarry)
+{
+#define AMX_GB(K, V, D, P) reinterpret_cast<const void*>(&groupby_kernel<K, V, D, P>)
+#define AMX_GB_PACK(K, V, D) (nocarry ? AMX_GB(K, V, D, true) : AMX_GB(K, V, D, false))
+#define AMX_GB_DENSE(K, V) (dense ? AMX_GB_PACK(K, V, true) : AMX_GB_PACK(K, V, false))
+    if (kslab) return vslab ? AMX_GB_DENSE(true, true) : AMX_GB_DENSE(true, false);
+    return vslab ? AMX_GB_DENSE(false, true) : AMX_GB_DENSE(false, false);
+#undef AMX_GB_DENSE
+#undef AMX_GB_PACK
+#undef AMX_GB
 }
 
 static uint64_t align256(uint64_t x) { return (x + 255) & ~255ull; }
@@ -292,16 +382,22 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
     p.gcnt = reinterpret_cast<unsigned long long*>(w + L.counts);
     if (p.n) {
         if (vals->bits <= 32) {
+            const bool nocarry = vals->bits <= kGbNoCarryBits;
+            p.flush_every = gb_flush_every(vals->bits);
             const uint32_t slots = p.dense ? (1u << p.kbits) : kGbHashSlots;
             const size_t smem = 16ull * slots;
-            e = cudaFuncSetAttribute(groupby_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            const void* fn = gb_kernel(keys->format == AMX_SLAB, vals->format == AMX_SLAB, p.dense, nocarry);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return cuda_fail(e, "groupby: shared memory attribute");
             int per_sm = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, groupby_kernel, kGbThreads, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kGbThreads, smem);
             uint64_t grid = (uint64_t)(per_sm > 0 ? per_sm : 1) * sm_count();
             const uint64_t chunks = (p.n + kGbChunk - 1) / kGbChunk;
             if (grid > chunks) grid = chunks;
-            groupby_kernel<<<(unsigned)grid, kGbThreads, smem, s>>>(p);
+            if (tuning().max_ctas && grid > tuning().max_ctas) grid = tuning().max_ctas;
+            void* args[] = {&p};
+            e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kGbThreads), args, smem, s);
+            if (e != cudaSuccess) return cuda_fail(e, "groupby: aggregation launch");
         }
         else {
             groupby_wide_kernel<<<sm_count() * 8, 256, 0, s>>>(p);

@@ -131,12 +131,13 @@ amx_status amx_workspace_status(const void* workspace, void* stream);
  * fields mean "automatic".  staged_bytes: input bytes kept staged ahead of the compute warps
  * (sets the depth of the shared-memory ring); compact_stages: ring depth of compacting passes;
  * policy: 0 automatic, 1 the generic runtime-width kernel, 1 + id a compile-time-width kernel
- * (id = slab width for one column).  amx_set_tuning(NULL) restores the defaults. */
+ * (id = slab width for one column); max_ctas: cap on the persistent grid of the group-by
+ * aggregation (0: every CTA that fits).  amx_set_tuning(NULL) restores the defaults. */
 typedef struct {
     uint32_t staged_bytes;
     uint32_t compact_stages;
     int32_t policy;
-    uint32_t reserved;
+    uint32_t max_ctas;
 } amx_tuning;
 amx_status amx_set_tuning(const amx_tuning* t);
 amx_status amx_get_tuning(amx_tuning* t);

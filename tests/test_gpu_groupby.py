@@ -80,3 +80,47 @@ def test_groupby_with_mask(cuda):
     assert np.array_equal(gpu_bytes(ok, g).view(np.uint32), present.astype(np.uint32))
     assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), want_sum[present])
     assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), want_cnt[present])
+
+
+@pytest.mark.parametrize("kf,kb,vf,vb", [
+    (SLAB, 10, SLAB, 16),     # dense table without carry words: flushed every 2^16 elements
+    (SLAB, 16, SLAB, 18),     # hash table without carry words: flushed every chunk (2^14)
+    (SLAB, 10, PLAIN32, 32),  # dense table, 32-bit sums with carry words
+    (NOGAPS, 9, SLAB, 21),    # general key reader, carry words
+    (PLAIN32, 12, NOGAPS, 3),  # general readers on both columns
+])
+def test_groupby_one_cta_flushes(cuda, kf, kb, vf, vb):
+    """One CTA aggregates 2^20 + 12345 elements, so its shared table is flushed mid-column
+    whenever a carry-free 32-bit sum could otherwise wrap: values at the top of their range on
+    one hot key reach the largest sums and counts the shared fields must hold."""
+    import ctypes as C
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = (1 << 20) + 12345
+    rng = np.random.default_rng(kb * 1000 + vb)
+    keys = rng.integers(0, 1 << kb, size=n, dtype=np.uint64)
+    keys[rng.random(n) < 0.8] = 5
+    vals = np.full(n, (1 << vb) - 1, np.uint64)
+    low = rng.random(n) < 0.1
+    vals[low] = rng.integers(0, 1 << vb, size=int(low.sum()), dtype=np.uint64)
+    kv, kraw = make_column(1, kf, kb, n, vals=keys)
+    vv, vraw = make_column(2, vf, vb, n, vals=vals)
+    want_sum = np.zeros(1 << kb, np.uint64)
+    want_cnt = np.zeros(1 << kb, np.uint64)
+    np.add.at(want_sum, kv.astype(np.int64), vv)
+    np.add.at(want_cnt, kv.astype(np.int64), 1)
+    t = A.Tuning(0, 0, 0, 1)
+    A.check(A.lib().amx_set_tuning(C.byref(t)))
+    try:
+        ok, osum, ocnt, ng = ops.groupby(to_gpu(kraw, n, kf, kb), to_gpu(vraw, n, vf, vb), key_fmt=PLAIN32)
+        g = int(ng[0].item())
+    finally:
+        A.check(A.lib().amx_set_tuning(None))
+    present = np.nonzero(want_cnt)[0]
+    assert want_cnt[5] > (1 << 19)
+    assert g == len(present)
+    assert np.array_equal(gpu_bytes(ok, g).view(np.uint32), present.astype(np.uint32))
+    assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), want_sum[present])
+    assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), want_cnt[present])
