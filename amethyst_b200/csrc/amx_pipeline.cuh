@@ -514,21 +514,23 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 bool done = false;
                 if constexpr (Pol::kSwar) {
                     // the usual compressstore: slabs of the input width in, slabs of it out
-                    if (p.out.format == AMX_SLAB && p.out.bits == (uint32_t)Pol::kBits) {
-                        if (cv16)
+                    if (Pol::kPlain || (p.out.format == AMX_SLAB && p.out.bits == (uint32_t)Pol::kBits)) {
+                        if (Pol::kPlain || cv16)
                             encode_slab_ct<Pol::kBits, uint16_t>(p.out, reinterpret_cast<const uint16_t*>(sv),
                                                                 slot_total[q], slot_g[q], tile == p.num_tiles - 1,
                                                                 etid, 32 * kEncoderWarps);
-                        else
+                        else if constexpr (!Pol::kPlain)
                             encode_slab_ct<Pol::kBits, uint32_t>(p.out, reinterpret_cast<const uint32_t*>(sv),
                                                                 slot_total[q], slot_g[q], tile == p.num_tiles - 1,
                                                                 etid, 32 * kEncoderWarps);
                         done = true;
                     }
                 }
-                if (!done)
-                    encode_any<V>(p.out, sv, cv16, slot_total[q], slot_g[q], tile == p.num_tiles - 1, etid,
-                                  32 * kEncoderWarps);
+                if constexpr (!Pol::kPlain) {
+                    if (!done)
+                        encode_any<V>(p.out, sv, cv16, slot_total[q], slot_g[q], tile == p.num_tiles - 1, etid,
+                                      32 * kEncoderWarps);
+                }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&cvfree[q]);
                 if (++q == NB) {
@@ -587,7 +589,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             for (int i = 0; i < SPT; i++) c += __popcll(g[i]);
             my_count += c;
 
-            if (p.mask_out) {
+            if (!Pol::kPlain && p.mask_out) {
                 uint64_t fl = 0;
 #pragma unroll
                 for (int i = 0; i < SPT; i++)
@@ -603,7 +605,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
 
             uint32_t pos = 0;
             uint8_t* slot = cv;
-            if (p.has_out) {  // compacting: block scan, publish, hand the tile to the look-back
+            if (Pol::kPlain || p.has_out) {  // compacting: block scan, publish, hand the tile to the look-back
                 volatile uint32_t* wt = warp_tot + 16 * (j & 1);
                 const uint32_t incl = warp_incl_scan<uint32_t>(c);
                 if (lane == 31) wt[warp] = incl;
@@ -620,7 +622,13 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 }
                 slot = cv + (size_t)q * p.slot_bytes;
             }
-            if (p.has_out || p.has_agg) {
+            if constexpr (Pol::kPlain) {
+                const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
+                uint64_t a = 0;
+                swar_visit<B, SPT, uint16_t, true, false>(x, g, 25 * wc > 32 * (uint32_t)R,
+                                                          reinterpret_cast<uint16_t*>(slot), pos, 0, a);
+            }
+            else if (p.has_out || p.has_agg) {
                 // the walk over set bits wins only below ~4% survivors in the warp
                 const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
                 const bool dense = 25 * wc > 32 * (uint32_t)R;
@@ -644,7 +652,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 }
                 if (p.has_agg) my_agg = agg_combine(p.agg, my_agg, a);
             }
-            if (p.has_out) {
+            if (Pol::kPlain || p.has_out) {
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&scat[q]);  // this warp's survivors are in slot q
                 if (++q == NB) {
@@ -652,7 +660,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     qphase ^= 1;
                 }
             }
-            if (p.mask_out) {
+            if (!Pol::kPlain && p.mask_out) {
                 compute_bar();
                 const uint32_t words = (valid + 31) / 32;
                 for (uint32_t i = tid; i < words; i += T) {
@@ -1010,6 +1018,7 @@ struct GenericPol {
     static constexpr int R = 8;
     static constexpr bool kWarpMajor = true;
     static constexpr bool kSwar = false;
+    static constexpr bool kPlain = false;
     static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;
 

@@ -79,6 +79,7 @@ struct SlabPol {
     static constexpr int R = EPS * SPT;
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = false;
+    static constexpr bool kPlain = false;
     // one CTA per SM: 16 compute warps, or 8 for the register-heavy 64-element runs and for
     // widths >= 17 (10+ slabs per thread: a 16-warp tile would not fit twice in shared memory)
     static constexpr uint32_t kCompute = (R > 40 || B >= 17) ? 256 : 512;
@@ -130,6 +131,7 @@ struct Slab2Pol {
     static constexpr int SB = R / EB;
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = false;
+    static constexpr bool kPlain = false;
     static constexpr uint32_t kCompute = R > 40 ? 256 : 512;
     static constexpr int kMinBlocks = 1;
     static_assert(R <= 64, "run too long for the flag word");

@@ -49,8 +49,11 @@ __host__ __device__ constexpr uint64_t swar_top_bits(int b)
 }
 
 // One slab column of width B with a predicate, evaluated field-parallel.  Each compute thread
-// owns SPT consecutive slabs of a tile (R = SPT * eps elements, R <= 64).
-template <int B>
+// owns SPT consecutive slabs of a tile (R = SPT * eps elements, R <= 64).  PLAIN: the request is
+// known to be the plain compressstore (slabs of width B <= 16 out, 16-bit gathered values, no
+// aggregate, no bitmask), so the kernel carries only that path: less code for the instruction
+// cache to hold next to the other warp roles.
+template <int B, bool PLAIN = false>
 struct SwarPol {
     using V = uint32_t;
     static constexpr int kBits = B;
@@ -59,11 +62,13 @@ struct SwarPol {
     static constexpr int R = EPS * SPT;
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = true;
+    static constexpr bool kPlain = PLAIN;
     static constexpr uint32_t kCompute = 512;
     static constexpr int kMinBlocks = 1;
     static constexpr uint64_t kField = (1ull << B) - 1;  // one field
     static constexpr uint64_t kTop = swar_top_bits(B);    // the top bit of every field
     static_assert(R <= 64, "a thread's run must fit one 64-bit flag word");
+    static_assert(!PLAIN || B <= 16, "the plain compressstore gathers 16-bit values");
 };
 
 // g[i] = in-place flags of word x[i] for the interval test selected by the template flags

@@ -584,7 +584,8 @@ def run_gpu(args):
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["batched_512"] = {"error": str(e)}
             for name, kw in [("chain_50pct", {"thresh": 4160}), ("chain_plain32_in", {"a_fmt": 0, "b_fmt": 0}),
-                             ("chain_plain32_out", {"out_fmt": 0})]:
+                             ("chain_plain32_out", {"out_fmt": 0}),
+                             ("chain_plain32_in_out", {"a_fmt": 0, "b_fmt": 0, "out_fmt": 0})]:
                 s2, ab2, st2, ib2 = chain_workload(dev, **kw)
                 tot2, per2 = time_steps(s2, max(3, min(args.steps, 50)), 3, stream)
                 c2 = int(st2["cnt"][0].item())
