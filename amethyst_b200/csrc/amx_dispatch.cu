@@ -88,6 +88,15 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
         swar_setup(p);
         return launch_swar((uint32_t)(id - kSwarPolicyBase), p, ws, ws_bytes, stream);
     }
+    if (plain_compacting(p)) {  // the two-column policies' variants that carry only this path
+        switch (id) {
+#define AMX_PLAIN_CASE(id, a, b) \
+    case id: return launch<Slab2Pol<a, b, true>>(p, ws, ws_bytes, stream);
+            AMX_SLAB2_PAIRS(AMX_PLAIN_CASE)
+#undef AMX_PLAIN_CASE
+            default: break;
+        }
+    }
     switch (id) {
 #define AMX_POLICY_CASE(id, Pol) \
     case id: return launch<Pol>(p, ws, ws_bytes, stream);

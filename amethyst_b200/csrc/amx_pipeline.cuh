@@ -531,6 +531,10 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                         encode_any<V>(p.out, sv, cv16, slot_total[q], slot_g[q], tile == p.num_tiles - 1, etid,
                                       32 * kEncoderWarps);
                 }
+                else if constexpr (!Pol::kSwar) {
+                    encode_tile<uint16_t>(p.out, reinterpret_cast<const uint16_t*>(sv), slot_total[q], slot_g[q],
+                                          tile == p.num_tiles - 1, etid, 32 * kEncoderWarps);
+                }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&cvfree[q]);
                 if (++q == NB) {
@@ -692,7 +696,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         uint64_t fl;
         Pol::decode(p, st, sbase + 3 * s, e0, v, fl);
         // element of flag bit i: thread-contiguous tid*R + i, warp-major warp*32R + 32i + lane
-        if (p.has_mask_in) {
+        if (!Pol::kPlain && p.has_mask_in) {
             const uint32_t* mw = reinterpret_cast<const uint32_t*>(st + p.m_off);
             if (WM) {
                 uint64_t mfl = 0;
@@ -733,7 +737,13 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         // gather then visit the survivors only (set bits of fl) instead of all R elements
         const bool sparse = !WM && __all_sync(0xffffffffu, __popcll(fl) <= kSparseMax);
 
-        if (p.has_agg && !sparse) {
+        if (Pol::kPlain && p.has_agg && !sparse) {  // a sum
+            uint64_t a = 0;
+#pragma unroll
+            for (int i = 0; i < R; i++) a += ((fl >> i) & 1) ? (uint64_t)v[i] : 0;
+            my_agg += a;
+        }
+        else if (!Pol::kPlain && p.has_agg && !sparse) {
             uint64_t a = 0;
             switch (p.agg) {
                 case AMX_AGG_SUM:
@@ -776,7 +786,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 bal[i] = __ballot_sync(0xffffffffu, (fl >> i) & 1);
                 c += __popc(bal[i]);
             }
-            if (p.mask_out) {
+            if (!Pol::kPlain && p.mask_out) {
                 uint32_t word = 0;
 #pragma unroll
                 for (int i = 0; i < R; i++)
@@ -787,7 +797,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         }
         else {
             c = __popcll(fl);
-            if (p.mask_out && fl) {
+            if (!Pol::kPlain && p.mask_out && fl) {
                 const uint32_t le0 = tid * R;
                 const uint32_t wi = le0 >> 5, sh = le0 & 31;
                 atomicOr(&bitmap[wi], (uint32_t)(fl << sh));
@@ -797,7 +807,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         }
         my_count += WM ? (lane == 0 ? c : 0) : c;
 
-        if (p.has_out) {
+        if (Pol::kPlain || p.has_out) {
             // block scan: survivors before this thread (or warp) inside the tile
             volatile uint32_t* wt = warp_tot + 16 * (j & 1);
             uint32_t pos, total = 0, before = 0;
@@ -820,7 +830,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 pos = before + incl - c;
             }
             uint8_t* slot = cv;
-            if (compact) {
+            if (Pol::kPlain || compact) {
                 // publish this tile's survivor count for the other CTAs' look-backs at once ...
                 if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
                 // ... but reuse slot q only after the encoder warps are done with its last tile
@@ -844,24 +854,34 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 uint64_t a = 0;
                 for (uint64_t f = fl; f; f &= f - 1) {
                     const V x = Pol::value_at(p, st, sbase + 3 * s, e0, __ffsll((long long)f) - 1);
-                    cv_put<V>(slot, cv16, pos++, x);
-                    a = agg_combine(p.agg, a, agg_encode(p.agg, (uint64_t)x));
+                    if constexpr (Pol::kPlain) {
+                        reinterpret_cast<uint16_t*>(slot)[pos++] = (uint16_t)x;
+                        a += x;
+                    }
+                    else {
+                        cv_put<V>(slot, cv16, pos++, x);
+                        a = agg_combine(p.agg, a, agg_encode(p.agg, (uint64_t)x));
+                    }
                 }
-                if (p.has_agg) my_agg = agg_combine(p.agg, my_agg, a);
+                if (Pol::kPlain) {
+                    if (p.has_agg) my_agg += a;
+                }
+                else if (p.has_agg)
+                    my_agg = agg_combine(p.agg, my_agg, a);
             }
-            else if (cv16) {
+            else if (Pol::kPlain || cv16) {
                 uint16_t* dst = reinterpret_cast<uint16_t*>(slot) + pos;
 #pragma unroll
                 for (int i = 0; i < R; i++)
                     if ((fl >> i) & 1) *dst++ = (uint16_t)v[i];
             }
-            else {
+            else if constexpr (!Pol::kPlain) {
                 V* dst = reinterpret_cast<V*>(slot) + pos;
 #pragma unroll
                 for (int i = 0; i < R; i++)
                     if ((fl >> i) & 1) *dst++ = v[i];
             }
-            if (compact) {
+            if (Pol::kPlain || compact) {
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&scat[q]);  // this warp's survivors are in slot q
                 if (++q == NB) {
@@ -869,14 +889,14 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     qphase ^= 1;
                 }
             }
-            else {  // element-wise output: the offset is known, encode right away
+            else if constexpr (!Pol::kPlain) {  // element-wise output: the offset is known, encode right away
                 compute_bar();
                 encode_any<V>(p.out, cv, cv16, total, e0, tile == p.num_tiles - 1, tid, T);
                 compute_bar();
             }
         }
         if (!WM) {
-            if (!p.has_out && p.has_agg && sparse) {
+            if (!Pol::kPlain && !p.has_out && p.has_agg && sparse) {
                 uint64_t a = 0;
                 for (uint64_t f = fl; f; f &= f - 1) {
                     const V x = Pol::value_at(p, st, sbase + 3 * s, e0, __ffsll((long long)f) - 1);
@@ -887,7 +907,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
         }
-        if (!WM && p.mask_out) {
+        if (!Pol::kPlain && !WM && p.mask_out) {
             compute_bar();
             const uint32_t words = (valid + 31) / 32;
             for (uint32_t i = tid; i < words; i += T) {

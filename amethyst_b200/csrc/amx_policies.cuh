@@ -120,7 +120,9 @@ __device__ __forceinline__ void combine_slabs(const uint64_t (&w)[N], uint32_t (
             v[j * EPS + k] = f(v[j * EPS + k], (uint32_t)((w[j] >> (k * B)) & ((1ull << B) - 1)));
 }
 
-template <int BA, int BB>
+// PLAIN: the request is known to be a compacting pass with 16-bit gathered values, no input
+// mask, no bitmask out and at most a sum, so the kernel carries only that path.
+template <int BA, int BB, bool PLAIN = false>
 struct Slab2Pol {
     using V = uint32_t;
     static constexpr int EA = 64 / BA;
@@ -131,7 +133,7 @@ struct Slab2Pol {
     static constexpr int SB = R / EB;
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = false;
-    static constexpr bool kPlain = false;
+    static constexpr bool kPlain = PLAIN;
     static constexpr uint32_t kCompute = R > 40 ? 256 : 512;
     static constexpr int kMinBlocks = 1;
     static_assert(R <= 64, "run too long for the flag word");
@@ -211,6 +213,14 @@ inline bool swar_applicable(const PipeParams& p)
 {
     return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && p.has_pred && !p.has_mask_in &&
            (!p.has_out || p.compact) && p.op == AMX_OP_LHS && !p.need_vmask && p.vbits <= 32;
+}
+
+// A request the PLAIN variants serve: compacting, 16-bit values, no input mask, no bitmask out,
+// no aggregate or a sum.
+inline bool plain_compacting(const PipeParams& p)
+{
+    return p.has_out && p.compact && !p.has_mask_in && !p.mask_out && p.vbits <= 16 &&
+           (!p.has_agg || p.agg == AMX_AGG_SUM);
 }
 
 // Policy for a request: the field-parallel policy when it applies, else compile-time widths
