@@ -90,10 +90,10 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
     }
     if (plain_compacting(p)) {  // the two-column policies' variants that carry only this path
         switch (id) {
-#define AMX_PLAIN_CASE(id, a, b) \
-    case id: return launch<Slab2Pol<a, b, true>>(p, ws, ws_bytes, stream);
+#define AMX_PLAIN_CASE(id, a, b) case id:
             AMX_SLAB2_PAIRS(AMX_PLAIN_CASE)
 #undef AMX_PLAIN_CASE
+            return launch_plain_pair(id, p, ws, ws_bytes, stream);
             default: break;
         }
     }

@@ -47,6 +47,9 @@ int sm_count();
 
 amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t stream);
 
+// plain compacting two-column policy `id` (amx_pairs.cu): one kernel per pair and cheap op
+amx_status launch_plain_pair(int id, PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream);
+
 // field-parallel slab policy (amx_swar.cu): predicate constants, and the launch for width `bits`
 void swar_setup(PipeParams& p);
 amx_status launch_swar(uint32_t bits, PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream);

@@ -120,9 +120,26 @@ __device__ __forceinline__ void combine_slabs(const uint64_t (&w)[N], uint32_t (
             v[j * EPS + k] = f(v[j * EPS + k], (uint32_t)((w[j] >> (k * B)) & ((1ull << B) - 1)));
 }
 
+// One of the cheap element-wise ops of the two-column policies, fixed at compile time.
+template <int OP>
+struct OpFn {
+    __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const
+    {
+        if constexpr (OP == AMX_OP_ADD) return a + b;
+        else if constexpr (OP == AMX_OP_SUB) return a - b;
+        else if constexpr (OP == AMX_OP_MUL) return a * b;
+        else if constexpr (OP == AMX_OP_MIN) return a < b ? a : b;
+        else if constexpr (OP == AMX_OP_MAX) return a > b ? a : b;
+        else if constexpr (OP == AMX_OP_AND) return a & b;
+        else if constexpr (OP == AMX_OP_OR) return a | b;
+        else return a ^ b;
+    }
+};
+
 // PLAIN: the request is known to be a compacting pass with 16-bit gathered values, no input
-// mask, no bitmask out and at most a sum, so the kernel carries only that path.
-template <int BA, int BB, bool PLAIN = false>
+// mask, no bitmask out and at most a sum, so the kernel carries only that path.  OP >= 0: the
+// element-wise op is fixed too (one of the eight cheap ops); -1: chosen at run time.
+template <int BA, int BB, bool PLAIN = false, int OP = -1>
 struct Slab2Pol {
     using V = uint32_t;
     static constexpr int EA = 64 / BA;
@@ -152,7 +169,10 @@ struct Slab2Pol {
             const uint64_t* w = reinterpret_cast<const uint64_t*>(st + p.b_off) + (first / EB - sb[1] / 8);
             uint64_t s[SB];
             lds_words<SB>(w, s);
-            switch (p.op) {
+            if constexpr (OP >= 0) {
+                combine_slabs<BB, EB, SB, R>(s, v, OpFn<OP>{});
+            }
+            else switch (p.op) {
                 case AMX_OP_ADD: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a + b; }); break;
                 case AMX_OP_SUB: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a - b; }); break;
                 case AMX_OP_MUL: combine_slabs<BB, EB, SB, R>(s, v, [](uint32_t a, uint32_t b) { return a * b; }); break;
@@ -178,7 +198,8 @@ struct Slab2Pol {
         const uint32_t a = (uint32_t)((wa[ja] >> (ka * BA)) & ((1ull << BA) - 1));
         const uint32_t b = (uint32_t)((wb[jb] >> (kb * BB)) & ((1ull << BB) - 1));
         uint32_t x;
-        switch (p.op) {
+        if constexpr (OP >= 0) x = OpFn<OP>{}(a, b);
+        else switch (p.op) {
             case AMX_OP_ADD: x = a + b; break;
             case AMX_OP_SUB: x = a - b; break;
             case AMX_OP_MUL: x = a * b; break;
