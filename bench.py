@@ -553,7 +553,7 @@ def run_gpu(args):
         "hbm_frac": round(byts / (ms * 1e-3) / 1e9 / peak, 4),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "amx::pipe_kernel<Slab2Pol<7,13>>", "alg_bytes_per_launch": byts,
+                     "kernel": "amx::pipe_kernel<Slab2Pol<7,13,true,AMX_OP_ADD>>", "alg_bytes_per_launch": byts,
                      "launch_ms": round(kern_ms, 5)},
         "gpu_launches": args.steps,
         "clocks": sampler.summary(),
