@@ -532,8 +532,18 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                                       32 * kEncoderWarps);
                 }
                 else if constexpr (!Pol::kSwar) {
-                    encode_tile<uint16_t>(p.out, reinterpret_cast<const uint16_t*>(sv), slot_total[q], slot_g[q],
-                                          tile == p.num_tiles - 1, etid, 32 * kEncoderWarps);
+                    const uint16_t* sv16 = reinterpret_cast<const uint16_t*>(sv);
+                    const bool last = tile == p.num_tiles - 1;
+                    if constexpr (Pol::kOutBits >= 1 && Pol::kOutBits <= 16) {
+                        if (p.out.format == AMX_SLAB && p.out.bits == (uint32_t)Pol::kOutBits)
+                            encode_slab_ct<Pol::kOutBits, uint16_t>(p.out, sv16, slot_total[q], slot_g[q], last, etid,
+                                                                   32 * kEncoderWarps);
+                        else
+                            encode_tile<uint16_t>(p.out, sv16, slot_total[q], slot_g[q], last, etid, 32 * kEncoderWarps);
+                    }
+                    else {
+                        encode_tile<uint16_t>(p.out, sv16, slot_total[q], slot_g[q], last, etid, 32 * kEncoderWarps);
+                    }
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&cvfree[q]);

@@ -136,6 +136,15 @@ struct OpFn {
     }
 };
 
+// Width of op(a, b) for a-bit and b-bit operands (amx_binary_out_bits for the cheap ops).
+constexpr int op_out_bits(int op, int a, int b)
+{
+    return op == AMX_OP_ADD ? (a > b ? a : b) + 1
+           : op == AMX_OP_MUL ? a + b
+           : (op == AMX_OP_MIN || op == AMX_OP_AND) ? (a < b ? a : b)
+                                                    : (a > b ? a : b);
+}
+
 // PLAIN: the request is known to be a compacting pass with 16-bit gathered values, no input
 // mask, no bitmask out and at most a sum, so the kernel carries only that path.  OP >= 0: the
 // element-wise op is fixed too (one of the eight cheap ops); -1: chosen at run time.
@@ -151,6 +160,8 @@ struct Slab2Pol {
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = false;
     static constexpr bool kPlain = PLAIN;
+    // output width the encoder warps pack at compile time (slabs of the op's natural width)
+    static constexpr int kOutBits = OP >= 0 ? op_out_bits(OP, BA, BB) : 0;
     static constexpr uint32_t kCompute = R > 40 ? 256 : 512;
     static constexpr int kMinBlocks = 1;
     static_assert(R <= 64, "run too long for the flag word");
