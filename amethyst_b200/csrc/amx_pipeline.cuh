@@ -583,7 +583,11 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             {
                 const uint8_t* st = stage0 + s * p.stage_bytes;
                 const uint64_t first = tile * (uint64_t)(T * SPT) + tid * SPT;  // first slab of this thread
-                lds_words<SPT>(reinterpret_cast<const uint64_t*>(st + p.a_off) + (first - sbase[3 * s] / 8), x);
+                const uint64_t* src = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first - sbase[3 * s] / 8);
+                if constexpr (Pol::kPlain && SPT == 8)
+                    lds_words8_rot(src, x);  // tiles fall on 32 KB boundaries: 64-byte-aligned runs
+                else
+                    lds_words<SPT>(src, x);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);  // the words are in registers: stage s is free

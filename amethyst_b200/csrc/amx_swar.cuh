@@ -40,6 +40,29 @@ __device__ __forceinline__ void lds_words(const uint64_t* src, uint64_t (&w)[N])
     }
 }
 
+// The 8 consecutive 64-bit words of this thread, for threads that own 64 contiguous bytes each
+// (src 128-byte aligned for even lanes).  Read as four 16-byte chunks in the natural order, the
+// 8 lanes of a quarter warp would hit only two 16-byte bank groups (a 4-way conflict); lane pair
+// r = (lane / 2) mod 4 reads its chunks rotated by r instead, so the quarter warp covers all 8
+// groups, and two register selects per chunk rotate them back.
+__device__ __forceinline__ void lds_words8_rot(const uint64_t* src, uint64_t (&w)[8])
+{
+    const uint32_t r = (threadIdx.x >> 1) & 3;
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4 t[4], u[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) t[k] = s[(k + r) & 3];  // t[k] = chunk (k + r) mod 4
+#pragma unroll
+    for (int c = 0; c < 4; c++) u[c] = (r & 1) ? t[(c + 3) & 3] : t[c];  // u[c] = t[c - (r & 1)]
+#pragma unroll
+    for (int c = 0; c < 4; c++) t[c] = (r & 2) ? u[(c + 2) & 3] : u[c];  // t[c] = chunk c
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        w[2 * c] = ((uint64_t)t[c].y << 32) | t[c].x;
+        w[2 * c + 1] = ((uint64_t)t[c].w << 32) | t[c].z;
+    }
+}
+
 // the top bit of each of the floor(64/b) fields of a slab word
 __host__ __device__ constexpr uint64_t swar_top_bits(int b)
 {
