@@ -68,7 +68,9 @@ amx_status launch(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream)
     // several tiles.  16-bit slots when the values fit.
     p.cv16 = p.has_out && p.vbits <= 16 ? 1 : 0;
     p.slot_bytes = round_up(TILE * (p.cv16 ? 2u : (uint32_t)sizeof(V)), 128);
-    const uint32_t budget = Pol::kMinBlocks >= 2 ? 110 * 1024 : 220 * 1024;
+    // shared memory to plan with: the whole 227 KB for the 24-compute-warp kernels (their tiles
+    // are 1.5 times larger), else 220 KB
+    const uint32_t budget = Pol::kMinBlocks >= 2 ? 110 * 1024 : (Pol::kCompute > 512 ? 227 * 1024 : 220 * 1024);
     const bool compact = p.has_out && p.compact;
     p.slots = p.has_out ? 1 : 0;
     if (compact) {

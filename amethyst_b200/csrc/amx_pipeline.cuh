@@ -342,11 +342,11 @@ __device__ __forceinline__ void wait_or_flag(uint64_t* bar, uint32_t parity, uin
 //   [0,64) full[8]  [64,128) empty[8]  [128,160) agg[4]  [160,192) gready[4]  [192,224) scat[4]
 //   [224,256) cvfree[4]                                                        (mbarriers)
 //   [256,320)  tickets[8]              [320,512) stage base offsets [8][3]
-//   [512,640)  warp totals [2][16]     [640,768) warp counts [16]  [768,848) per-slot tile / total / offset
-//   [896,1024) warp aggregates [16]    [1024,5120) tile bitmap (thread-contiguous policies)
+//   [512,768)  warp totals [2][32]     [768,1024) warp counts [32]  [1024,1280) warp aggregates [32]
+//   [1280,1360) per-slot tile / total / offset                     [1536,5632) tile bitmap (thread-contiguous policies)
 //   [kCvOff, smem_fixed)  gathered-value slots;  [smem_fixed, ...) p.stages stage buffers
-constexpr uint32_t kBitmapOff = 1024;
-constexpr uint32_t kCvOff = 5120;
+constexpr uint32_t kBitmapOff = 1536;
+constexpr uint32_t kCvOff = 5632;
 constexpr uint64_t kNoTile = ~0ull;
 constexpr uint32_t kEncoderWarps = 4;
 constexpr int kSparseMax = 3;  // survivors per thread up to which a warp gathers sparsely
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     constexpr uint32_t NW = T / 32;
     constexpr uint32_t TILE = T * R;
     static_assert(TILE / 32 * 4 <= kCvOff - kBitmapOff, "bitmap region");
-    static_assert(NW <= 16, "warp arrays hold 16 compute warps");
+    static_assert(NW <= 32, "warp arrays hold 32 compute warps");
     static_assert(!WM || R <= 32, "warp-major runs keep one ballot per lane");
     auto compute_bar = []() { compute_bar_n<T>(); };
 
@@ -397,11 +397,11 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     volatile uint64_t* tickets = reinterpret_cast<volatile uint64_t*>(smem + 256);
     uint64_t* sbase = reinterpret_cast<uint64_t*>(smem + 320);
     volatile uint32_t* warp_tot = reinterpret_cast<volatile uint32_t*>(smem + 512);
-    uint64_t* warp_cnt = reinterpret_cast<uint64_t*>(smem + 640);
-    volatile uint64_t* slot_tile = reinterpret_cast<volatile uint64_t*>(smem + 768);
-    volatile uint32_t* slot_total = reinterpret_cast<volatile uint32_t*>(smem + 800);
-    volatile uint64_t* slot_g = reinterpret_cast<volatile uint64_t*>(smem + 816);
-    uint64_t* warp_agg = reinterpret_cast<uint64_t*>(smem + 896);
+    uint64_t* warp_cnt = reinterpret_cast<uint64_t*>(smem + 768);
+    uint64_t* warp_agg = reinterpret_cast<uint64_t*>(smem + 1024);
+    volatile uint64_t* slot_tile = reinterpret_cast<volatile uint64_t*>(smem + 1280);
+    volatile uint32_t* slot_total = reinterpret_cast<volatile uint32_t*>(smem + 1312);
+    volatile uint64_t* slot_g = reinterpret_cast<volatile uint64_t*>(smem + 1328);
     uint32_t* bitmap = reinterpret_cast<uint32_t*>(smem + kBitmapOff);
     uint8_t* cv = smem + kCvOff;
     uint8_t* stage0 = smem + p.smem_fixed;
@@ -624,7 +624,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             uint32_t pos = 0;
             uint8_t* slot = cv;
             if (Pol::kPlain || p.has_out) {  // compacting: block scan, publish, hand the tile to the look-back
-                volatile uint32_t* wt = warp_tot + 16 * (j & 1);
+                volatile uint32_t* wt = warp_tot + 32 * (j & 1);
                 const uint32_t incl = warp_incl_scan<uint32_t>(c);
                 if (lane == 31) wt[warp] = incl;
                 compute_bar();
@@ -823,7 +823,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
 
         if (Pol::kPlain || p.has_out) {
             // block scan: survivors before this thread (or warp) inside the tile
-            volatile uint32_t* wt = warp_tot + 16 * (j & 1);
+            volatile uint32_t* wt = warp_tot + 32 * (j & 1);
             uint32_t pos, total = 0, before = 0;
             if (WM) {
                 if (lane == 0) wt[warp] = c;

@@ -86,7 +86,9 @@ struct SwarPol {
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = true;
     static constexpr bool kPlain = PLAIN;
-    static constexpr uint32_t kCompute = 512;
+    // the plain compressstore at widths of at most 5 fields per slab runs 24 compute warps (its
+    // registers allow 960 threads): more warps to hide the compute warps' latencies
+    static constexpr uint32_t kCompute = (PLAIN && EPS * SPT <= 40) ? 768 : 512;
     static constexpr int kMinBlocks = 1;
     static constexpr uint64_t kField = (1ull << B) - 1;  // one field
     static constexpr uint64_t kTop = swar_top_bits(B);    // the top bit of every field
