@@ -162,7 +162,12 @@ struct Slab2Pol {
     static constexpr bool kPlain = PLAIN;
     // output width the encoder warps pack at compile time (slabs of the op's natural width)
     static constexpr int kOutBits = OP >= 0 ? op_out_bits(OP, BA, BB) : 0;
-    static constexpr uint32_t kCompute = R > 40 ? 256 : 512;
+    // the plain variants run 20 compute warps where two stages and two slots of 16-bit values
+    // still fit in 227 KB of shared memory (5632 bytes of control data first)
+    static constexpr uint32_t kT20 = 640 * R;
+    static constexpr bool kFits20 =
+        5632u + 2u * (2u * kT20) + 2u * (8u * (kT20 / EA + 2) + 8u * (kT20 / EB + 2) + 352u) <= 227u * 1024u;
+    static constexpr uint32_t kCompute = R > 40 ? 256 : ((PLAIN && kFits20) ? 640 : 512);
     static constexpr int kMinBlocks = 1;
     static_assert(R <= 64, "run too long for the flag word");
 
