@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     // CTAs publish each count right after the tile's scan).  No tile waits on another tile's
     // look-back: there is no chain of inclusive prefixes across CTAs.
     if (warp == NW + 1) {
-        if (!Pol::kFilter && compact) {
+        if (!Pol::kFilter && !Pol::kAggOnly && compact) {
             uint64_t prev_tile = 0, prev_end = 0;
             bool first = true;
             for (uint32_t j = 0, q = 0, ph = 0;; j++) {
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     // Re-encode each slot's gathered survivors at the offset the look-back warp found, then
     // give the slot back to the compute warps.
     if (warp >= NW + 2) {
-        if (!Pol::kFilter && compact) {
+        if (!Pol::kFilter && !Pol::kAggOnly && compact) {
             const uint32_t etid = tid - (NW + 2) * 32;
             for (uint32_t j = 0, q = 0, ph = 0;; j++) {
                 wait_or_flag(&gready[q], ph, &p.ws->err);
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 const uint8_t* st = stage0 + s * p.stage_bytes;
                 const uint64_t first = tile * (uint64_t)(T * SPT) + tid * SPT;  // first slab of this thread
                 const uint64_t* src = reinterpret_cast<const uint64_t*>(st + p.a_off) + (first - sbase[3 * s] / 8);
-                if constexpr ((Pol::kPlain || Pol::kFilter) && SPT == 8)
+                if constexpr ((Pol::kPlain || Pol::kFilter || Pol::kAggOnly) && SPT == 8)
                     lds_words8_rot(src, x);  // tiles fall on 32 KB boundaries: 64-byte-aligned runs
                 else
                     lds_words<SPT>(src, x);
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             for (int i = 0; i < SPT; i++) c += __popcll(g[i]);
             my_count += c;
 
-            if (Pol::kFilter || (!Pol::kPlain && p.mask_out)) {
+            if (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out)) {
                 uint64_t fl = 0;
 #pragma unroll
                 for (int i = 0; i < SPT; i++)
@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
 
             uint32_t pos = 0;
             uint8_t* slot = cv;
-            if (!Pol::kFilter && (Pol::kPlain || p.has_out)) {  // compacting: block scan, publish, hand the tile to the look-back
+            if (!Pol::kFilter && !Pol::kAggOnly && (Pol::kPlain || p.has_out)) {  // compacting: block scan, publish, hand the tile to the look-back
                 volatile uint32_t* wt = warp_tot + 32 * (j & 1);
                 const uint32_t incl = warp_incl_scan<uint32_t>(c);
                 if (lane == 31) wt[warp] = incl;
@@ -641,6 +641,14 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 slot = cv + (size_t)q * p.slot_bytes;
             }
             if constexpr (Pol::kFilter) {
+            }
+            else if constexpr (Pol::kAggOnly) {
+                if (p.has_agg) {
+                    const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
+                    uint64_t a = 0;
+                    swar_visit<B, SPT, uint32_t, false, true>(x, g, 25 * wc > 32 * (uint32_t)R, nullptr, 0, p.agg, a);
+                    my_agg = agg_combine(p.agg, my_agg, a);
+                }
             }
             else if constexpr (Pol::kPlain) {
                 const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
@@ -672,7 +680,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 }
                 if (p.has_agg) my_agg = agg_combine(p.agg, my_agg, a);
             }
-            if (!Pol::kFilter && (Pol::kPlain || p.has_out)) {
+            if (!Pol::kFilter && !Pol::kAggOnly && (Pol::kPlain || p.has_out)) {
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&scat[q]);  // this warp's survivors are in slot q
                 if (++q == NB) {
@@ -680,7 +688,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     qphase ^= 1;
                 }
             }
-            if (Pol::kFilter || (!Pol::kPlain && p.mask_out)) {
+            if (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out)) {
                 compute_bar();
                 const uint32_t words = (valid + 31) / 32;
                 for (uint32_t i = tid; i < words; i += T) {
@@ -1056,6 +1064,7 @@ struct GenericPol {
     static constexpr bool kSwar = false;
     static constexpr bool kPlain = false;
     static constexpr bool kFilter = false;
+    static constexpr bool kAggOnly = false;
     static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;
 

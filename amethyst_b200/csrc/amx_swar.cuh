@@ -76,8 +76,8 @@ __host__ __device__ constexpr uint64_t swar_top_bits(int b)
 // known to be the plain compressstore (slabs of width B <= 16 out, 16-bit gathered values, no
 // aggregate, no bitmask), so the kernel carries only that path: less code for the instruction
 // cache to hold next to the other warp roles.  FILTER: likewise for a request that only writes
-// the bitmask.
-template <int B, bool PLAIN = false, bool FILTER = false>
+// the bitmask; AGGONLY: for one that only counts and aggregates.
+template <int B, bool PLAIN = false, bool FILTER = false, bool AGGONLY = false>
 struct SwarPol {
     using V = uint32_t;
     static constexpr int kBits = B;
@@ -87,10 +87,11 @@ struct SwarPol {
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = true;
     static constexpr bool kPlain = PLAIN;
-    static constexpr bool kFilter = FILTER;  // the request only writes the bitmask
+    static constexpr bool kFilter = FILTER;    // the request only writes the bitmask
+    static constexpr bool kAggOnly = AGGONLY;  // the request only counts and aggregates
     // the plain compressstore at widths of at most 5 fields per slab runs 24 compute warps (its
     // registers allow 960 threads): more warps to hide the compute warps' latencies
-    static constexpr uint32_t kCompute = ((PLAIN || FILTER) && EPS * SPT <= 40) ? 768 : 512;
+    static constexpr uint32_t kCompute = ((PLAIN || FILTER || AGGONLY) && EPS * SPT <= 40) ? 768 : 512;
     static constexpr int kMinBlocks = 1;
     static constexpr uint64_t kField = (1ull << B) - 1;  // one field
     static constexpr uint64_t kTop = swar_top_bits(B);    // the top bit of every field

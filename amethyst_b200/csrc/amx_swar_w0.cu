@@ -8,6 +8,8 @@ amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t 
 {
     if (!p.has_out && !p.has_agg && p.mask_out)  // the filter alone
         return launch<SwarPol<B, false, true>>(p, ws, ws_bytes, stream);
+    if (!p.has_out && !p.mask_out)  // a count and at most one aggregate
+        return launch<SwarPol<B, false, false, true>>(p, ws, ws_bytes, stream);
     if constexpr (B <= 16) {
         // the plain compressstore takes the kernel that carries only its own path
         if (p.has_out && p.compact && !p.has_agg && !p.mask_out && p.out.format == AMX_SLAB && p.out.bits == B &&

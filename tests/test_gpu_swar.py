@@ -104,3 +104,24 @@ def test_swar_chain_outputs(cuda, restore_tuning, bits, n):
                 assert np.array_equal(gm, O.filter(raw, n, SLAB, bits, op))
                 if out_fmt is not None:
                     assert np.array_equal(gpu_bytes(out, wcnt), wout), (bits, n, kind, out_fmt)
+
+
+@pytest.mark.parametrize("bits", [1, 5, 8, 11, 13, 16, 24, 32])
+@pytest.mark.parametrize("n", [0, 1, 4097, 32769, 300001])
+def test_swar_count_and_aggregate_only(cuda, restore_tuning, bits, n):
+    """Count and every aggregation with no output column and no bitmask (the count-and-aggregate
+    variant of the field-parallel kernel), automatic policy choice."""
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    v, raw = make_column(bits * 11 + n, SLAB, bits, n)
+    col = to_gpu(raw, n, SLAB, bits)
+    top = (1 << bits) - 1
+    for kind, k0, k1 in [(A.PRED_LT, top // 3 + 1, 0), (A.PRED_BETWEEN, top // 5, top // 2), (A.PRED_ALL, 0, 0)]:
+        p = ops.predicate(kind, k0, k1, bits)
+        op = O.pred(kind, k0, k1, bits)
+        for agg in range(6):
+            _, _, cnt, ag = ops.chain(col, None, A.OP_LHS, bits, p, agg)
+            _, wcnt, wagg = O.chain(A.OP_LHS, (raw, SLAB, bits), None, bits, op, agg, None, None, n)
+            assert int(cnt[0].item()) == wcnt, (bits, n, kind, agg)
+            assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (bits, n, kind, agg)
