@@ -255,10 +255,28 @@ def fc_1gib(dev, steps, warmup):
     c = int(cnt[0].item())
     byts = storage_bytes(2, 11, n) + storage_bytes(2, 11, c) + 8
     ms = total / steps
-    del col, out, ws
+    res = {"workload": "filter v<205 + compressstore, 1 GiB column of 11-bit slabs (671,088,640 elements)",
+           "GB_s": byts / (ms * 1e-3) / 1e9, "ms_per_step": ms, "selectivity": c / n, "alg_bytes": byts}
+    # the same column through the other two single-column operators: filter to a bitmask, and
+    # count + sum of the passing values
+    mask = torch.empty(ops.mask_words(n) + 4, dtype=torch.int32, device=dev)
+    agg = torch.zeros(2, dtype=torch.int64, device=dev)
+    desc = A.ChainDesc(A.OP_LHS, 11, pred, A.AGG_SUM, 0)
+    sp = lambda: C.c_void_p(torch.cuda.current_stream().cuda_stream)  # noqa: E731
+    for name, fn, extra_bytes in [
+        ("filter_to_bitmask", lambda: A.check(L.amx_filter(C.byref(cd), C.byref(pred), C.c_void_p(mask.data_ptr()),
+                                                           C.c_void_p(ws.data_ptr()), ws.numel(), sp())),
+         4 * ((n + 31) // 32)),
+        ("count_and_sum", lambda: A.check(L.amx_chain(C.byref(desc), C.byref(cd), None, None, None,
+                                                      C.c_void_p(cnt.data_ptr()), C.c_void_p(agg.data_ptr()),
+                                                      C.c_void_p(ws.data_ptr()), ws.numel(), sp())), 16)]:
+        t2, _ = time_steps(fn, steps, warmup, torch.cuda.current_stream())
+        ms2 = t2 / steps
+        b2 = storage_bytes(2, 11, n) + extra_bytes
+        res[name] = {"GB_s": round(b2 / (ms2 * 1e-3) / 1e9, 2), "ms_per_step": round(ms2, 5), "alg_bytes": b2}
+    del col, out, ws, mask
     torch.cuda.empty_cache()
-    return {"workload": "filter v<205 + compressstore, 1 GiB column of 11-bit slabs (671,088,640 elements)",
-            "GB_s": byts / (ms * 1e-3) / 1e9, "ms_per_step": ms, "selectivity": c / n, "alg_bytes": byts}
+    return res
 
 
 def batched_512(dev, steps):
