@@ -40,6 +40,8 @@ struct GbParams {
     uint32_t kbits;
     uint32_t dense;
     uint64_t flush_every;  // elements per CTA between flushes of its shared table
+    uint32_t run;          // groupby_phase_kernel: elements per thread and chunk
+    uint32_t pad;
     unsigned long long* gsum;
     unsigned long long* gcnt;
 };
@@ -280,6 +282,120 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
     }
 }
 
+// Slab keys and slab values, no mask: every thread's run starts on a slab boundary of BOTH
+// columns (run length a multiple of the two field counts' lcm), so all lanes of a warp reach
+// the end of a word at the same element.  The word after the current one is loaded as soon as
+// the current one is taken, a whole word of elements ahead of its use.
+struct PhaseRun {
+    const unsigned long long* w;
+    uint64_t cur;   // current word, shifted so that the next element sits in the low bits
+    uint64_t nxt;   // the word after it (0 past the column's end)
+    uint64_t wi;    // index of the current word
+    uint64_t nw;    // words in the column
+    uint32_t k;     // field of the next element
+};
+
+__device__ __forceinline__ PhaseRun phase_open(const ColDev& c, uint64_t e)
+{
+    PhaseRun r;
+    r.w = reinterpret_cast<const unsigned long long*>(c.data);
+    r.nw = c.bytes / 8;
+    r.wi = udiv64(e, c.magic64, c.eps);  // e is a multiple of eps
+    r.k = 0;
+    r.cur = r.wi < r.nw ? __ldg(r.w + r.wi) : 0;
+    r.nxt = r.wi + 1 < r.nw ? __ldg(r.w + r.wi + 1) : 0;
+    return r;
+}
+
+__device__ __forceinline__ uint32_t phase_next(const ColDev& c, PhaseRun& r)
+{
+    const uint32_t v = (uint32_t)r.cur & (uint32_t)c.mask;
+    r.cur >>= c.bits;
+    if (++r.k == c.eps) {  // the same element for every lane of the warp
+        r.k = 0;
+        r.cur = r.nxt;
+        ++r.wi;
+        r.nxt = r.wi + 1 < r.nw ? __ldg(r.w + r.wi + 1) : 0;
+    }
+    return v;
+}
+
+template <bool DENSE, bool NOCARRY>
+__global__ void __launch_bounds__(kGbThreads) groupby_phase_kernel(const __grid_constant__ GbParams p)
+{
+    extern __shared__ __align__(16) uint32_t tab[];
+    const uint32_t slots = DENSE ? (1u << p.kbits) : kGbHashSlots;
+    uint32_t* tkey = tab;
+    uint32_t* tlo = tab + slots;
+    uint32_t* thi = tab + 2 * slots;
+    uint32_t* tcnt = tab + 3 * slots;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t run = p.run;
+    const uint64_t chunk_elems = (uint64_t)kGbThreads * run;
+    const uint64_t nchunks = (p.n + chunk_elems - 1) / chunk_elems;
+
+    for (uint32_t i = tid; i < slots; i += blockDim.x) {
+        if (!DENSE) tkey[i] = kEmptyKey;
+        tlo[i] = thi[i] = tcnt[i] = 0;
+    }
+    __syncthreads();
+    uint64_t seen = 0;
+    for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        const uint64_t e0 = chunk * chunk_elems;
+        const uint64_t e1 = e0 + chunk_elems < p.n ? e0 + chunk_elems : p.n;
+        const uint64_t r0 = e0 + (uint64_t)tid * run;
+        const uint32_t rn = r0 >= e1 ? 0 : (uint32_t)(e1 - r0 < run ? e1 - r0 : run);
+        if (rn) {
+            PhaseRun kr = phase_open(p.k, r0);
+            PhaseRun vr = phase_open(p.v, r0);
+#pragma unroll 4
+            for (uint32_t i = 0; i < rn; i++) {
+                const uint32_t key = phase_next(p.k, kr);
+                const uint32_t val = phase_next(p.v, vr);
+                uint32_t slot = key;
+                if (!DENSE) {
+                    slot = gb_probe(tkey, key);
+                    if (slot == kEmptyKey) {  // table crowded: spill to the global table
+                        atomicAdd(&p.gsum[key], (unsigned long long)val);
+                        atomicAdd(&p.gcnt[key], 1ull);
+                        continue;
+                    }
+                }
+                if (NOCARRY) {
+                    atomicAdd(&tlo[slot], val);
+                    atomicAdd(&tcnt[slot], 1u);
+                }
+                else {
+                    const uint32_t old = atomicAdd(&tlo[slot], val);
+                    if (old + val < old) atomicAdd(&thi[slot], 1u);
+                    atomicAdd(&tcnt[slot], 1u);
+                }
+            }
+        }
+        // flush before the next chunk could take a field past its bound
+        seen += e1 - e0;
+        const bool last = chunk + gridDim.x >= nchunks;
+        if (last || seen + chunk_elems > p.flush_every) {
+            __syncthreads();
+            for (uint32_t i = tid; i < slots; i += blockDim.x) {
+                const uint32_t c = tcnt[i];
+                const uint64_t sum = NOCARRY ? tlo[i] : ((uint64_t)thi[i] << 32) | tlo[i];
+                if (c) {
+                    const uint32_t key = DENSE ? i : tkey[i];
+                    atomicAdd(&p.gsum[key], (unsigned long long)sum);
+                    atomicAdd(&p.gcnt[key], (unsigned long long)c);
+                }
+                if (!DENSE) tkey[i] = kEmptyKey;
+                tlo[i] = thi[i] = tcnt[i] = 0;
+            }
+            __syncthreads();
+            seen = 0;
+        }
+    }
+}
+
+static uint32_t gcd_u32(uint32_t a, uint32_t b) { return b ? gcd_u32(b, a % b) : a; }
+
 // Values wider than 32 bits: every element goes to the global table directly.
 __global__ void groupby_wide_kernel(const __grid_constant__ GbParams p)
 {
@@ -387,12 +503,28 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
             const uint32_t slots = p.dense ? (1u << p.kbits) : kGbHashSlots;
             const size_t smem = 16ull * slots;
             const void* fn = gb_kernel(keys->format == AMX_SLAB, vals->format == AMX_SLAB, p.dense, nocarry);
+            // slab keys and values without a mask: runs aligned to both columns' slabs, when
+            // their length (a multiple of the field counts' lcm) stays short and a chunk of them
+            // fits between two flushes
+            if (keys->format == AMX_SLAB && vals->format == AMX_SLAB && !d_mask) {
+                const uint32_t ek = p.k.eps, ev = p.v.eps;
+                const uint32_t l = ek / gcd_u32(ek, ev) * ev;
+                const uint32_t run = l <= 64 ? l * ((32 + l - 1) / l) : 0;
+                if (run && run <= 64 && (uint64_t)kGbThreads * run <= p.flush_every) {
+                    p.run = run;
+                    fn = p.dense ? (nocarry ? reinterpret_cast<const void*>(&groupby_phase_kernel<true, true>)
+                                            : reinterpret_cast<const void*>(&groupby_phase_kernel<true, false>))
+                                 : (nocarry ? reinterpret_cast<const void*>(&groupby_phase_kernel<false, true>)
+                                            : reinterpret_cast<const void*>(&groupby_phase_kernel<false, false>));
+                }
+            }
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return cuda_fail(e, "groupby: shared memory attribute");
             int per_sm = 0;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kGbThreads, smem);
             uint64_t grid = (uint64_t)(per_sm > 0 ? per_sm : 1) * sm_count();
-            const uint64_t chunks = (p.n + kGbChunk - 1) / kGbChunk;
+            const uint64_t chunk_elems = p.run ? (uint64_t)kGbThreads * p.run : kGbChunk;
+            const uint64_t chunks = (p.n + chunk_elems - 1) / chunk_elems;
             if (grid > chunks) grid = chunks;
             if (tuning().max_ctas && grid > tuning().max_ctas) grid = tuning().max_ctas;
             void* args[] = {&p};
