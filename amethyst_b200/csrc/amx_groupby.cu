@@ -16,6 +16,9 @@
 //    A CTA flushes its shared table into the dense global table of uint64 sums and counts
 //    (2^key_bits entries, 64-bit atomics) once, after its last chunk, or every 2^(32 - value
 //    bits) elements (carry-free sums, at most 2^30) before a 32-bit field could overflow.
+//    groupby_phase_kernel does the same for slab keys and slab values without a mask, with runs
+//    whose length is a multiple of both columns' field counts: the lanes of a warp then change
+//    words at the same element, and the next word is loaded a word ahead.
 // 2. the groups are extracted with the tile pipeline itself: mask = filter(count != 0), then
 //    compressstore of the key indices, the sums and the counts into the caller's output columns.
 #include "amx_dispatch.h"
@@ -41,7 +44,7 @@ struct GbParams {
     uint32_t dense;
     uint64_t flush_every;  // elements per CTA between flushes of its shared table
     uint32_t run;          // groupby_phase_kernel: elements per thread and chunk
-    uint32_t pad;
+    uint32_t pad;          // alignment of the pointers below
     unsigned long long* gsum;
     unsigned long long* gcnt;
 };
