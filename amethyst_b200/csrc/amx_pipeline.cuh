@@ -6,11 +6,14 @@
 //   * the loader warp (one lane) takes tiles from an atomic ticket counter and stages each
 //     tile's bytes of every input into a ring of 2..8 shared-memory stages with 1-D bulk
 //     copies (cp.async.bulk, completion on the stage's `full` mbarrier);
-//   * 16 compute warps decode R elements per thread straight from the staged packed words (a
-//     policy: field-parallel slab words, thread-contiguous compile-time-width readers, or
-//     warp-major runtime-width readers), apply the op and the predicate, build the bitmask /
-//     aggregate / count, scan the tile's survivors, publish the count for the look-back, and
-//     gather the survivors into one of up to four shared-memory slots;
+//   * 8 to 24 compute warps (Pol::kCompute) decode R elements per thread straight from the
+//     staged packed words (a policy: field-parallel slab words, thread-contiguous
+//     compile-time-width readers, or warp-major runtime-width readers), apply the op and the
+//     predicate, build the bitmask / aggregate / count, scan the tile's survivors, publish the
+//     count for the look-back, and gather the survivors into one of up to four shared-memory
+//     slots.  The request-specific policy variants (Pol::kPlain, kFilter, kAggOnly) compile only
+//     their request's path, which keeps the hot loop small in the instruction cache the compute
+//     warps share with the other roles, and frees the registers for more compute warps;
 //   * the look-back warp turns each tile's published count into its output offset: the CTA's
 //     tiles arrive in ticket order, so the offset is the end of the CTA's previous tile plus the
 //     counts of the tiles other CTAs took in between;
