@@ -507,6 +507,26 @@ def cpu_baseline_chain(st, threads):
     return dt, cnt, agg, (gc == cnt and ga == agg), in_bytes
 
 
+def job_time_ms(local_ms, dist=None, device=None):
+    """Whole-job time: the maximum of every rank's own device-timed total.  Every rank calls it
+    after its timed region; the barrier first keeps a rank from reading before all have
+    finished."""
+    if dist is None:
+        return float(local_ms)
+    import torch
+
+    dist.barrier()
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, bytes_per_rank, ms_per_step):
+    """Aggregate packed GB/s of the job: every rank processes its own copy of the workload per
+    step (replicas, weak scaling), so the job moves world x bytes_per_rank per step."""
+    return world * bytes_per_rank / (ms_per_step * 1e-3) / 1e9
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -542,15 +562,11 @@ def run_gpu(args):
     total_ms, per = time_steps(step, args.steps, 0, stream)
     sampler.stop()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = job_time_ms(total_ms, dist, dev)
     count = int(st["cnt"][0].item())
     ms = total_ms / args.steps
     byts = alg_bytes(count)
-    value = world * byts / (ms * 1e-3) / 1e9
+    value = job_value(world, byts, ms)
     peak, peak_kind = measured_peaks()
     kern_ms = statistics.mean(per)
     achieved = byts / (kern_ms * 1e-3) / 1e9
