@@ -19,8 +19,9 @@
 //    groupby_phase_kernel does the same for slab keys and slab values without a mask, with runs
 //    whose length is a multiple of both columns' field counts: the lanes of a warp then change
 //    words at the same element, and the next word is loaded a word ahead.
-// 2. the groups are extracted with the tile pipeline itself: mask = filter(count != 0), then
-//    compressstore of the key indices, the sums and the counts into the caller's output columns.
+// 2. the groups are extracted: for at most 4096 groups by one CTA (gb_extract_kernel), else with
+//    the tile pipeline itself: mask = filter(count != 0), then compressstore of the key indices,
+//    the sums and the counts into the caller's output columns.
 #include "amx_dispatch.h"
 #include "amx_pipeline.cuh"
 
@@ -411,6 +412,68 @@ __global__ void groupby_wide_kernel(const __grid_constant__ GbParams p)
     }
 }
 
+// Groups of a table of at most kGbExtractMax entries, extracted by one CTA: the present keys
+// (count != 0) in ascending order are compacted into shared memory with their sums and counts,
+// then encoded into the caller's output columns (any format), and their number is written to
+// d_groups.  One launch instead of the filter + three compressstores of the general path.
+constexpr uint32_t kGbExtractMax = 4096;
+constexpr uint32_t kGbExtractThreads = 1024;
+constexpr uint32_t kGbExtractSmem = kGbExtractMax * (4 + 8 + 8);
+
+__global__ void __launch_bounds__(kGbExtractThreads) gb_extract_kernel(const unsigned long long* gsum,
+                                                                       const unsigned long long* gcnt, uint32_t g,
+                                                                       OutDev ok, OutDev os, OutDev oc, uint32_t has,
+                                                                       uint64_t* d_groups)
+{
+    extern __shared__ __align__(16) uint8_t xs[];
+    uint64_t* sums = reinterpret_cast<uint64_t*>(xs);
+    uint64_t* cnts = sums + kGbExtractMax;
+    uint32_t* keys = reinterpret_cast<uint32_t*>(cnts + kGbExtractMax);
+    __shared__ uint32_t wtot[32];
+    constexpr uint32_t PER = kGbExtractMax / kGbExtractThreads;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint64_t c[PER];
+    uint32_t n = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < PER; j++) {
+        const uint32_t i = tid * PER + j;
+        c[j] = i < g ? gcnt[i] : 0;
+        n += c[j] != 0;
+    }
+    uint32_t incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) wtot[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = lane < 32 ? wtot[lane] : 0;  // every warp scans the 32 warp totals itself
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, wpre, o);
+        if (lane >= (uint32_t)o) wpre += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, wpre, 31);
+    const uint32_t before = warp ? __shfl_sync(0xffffffffu, wpre, warp - 1) : 0;
+    uint32_t pos = before + incl - n;
+#pragma unroll
+    for (uint32_t j = 0; j < PER; j++) {
+        if (c[j]) {
+            const uint32_t i = tid * PER + j;
+            keys[pos] = i;
+            sums[pos] = gsum[i];
+            cnts[pos] = c[j];
+            pos++;
+        }
+    }
+    __syncthreads();
+    if (has & 1) encode_tile<uint32_t>(ok, keys, total, 0, true, tid, kGbExtractThreads);
+    if (has & 2) encode_tile<uint64_t>(os, sums, total, 0, true, tid, kGbExtractThreads);
+    if (has & 4) encode_tile<uint64_t>(oc, cnts, total, 0, true, tid, kGbExtractThreads);
+    if (tid == 0 && d_groups) *d_groups = total;
+}
+
 __global__ void iota_kernel(uint32_t* out, uint64_t n)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -540,6 +603,22 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: aggregation launch");
     }
     // groups: keys with a nonzero count, ascending
+    if (g <= kGbExtractMax) {
+        OutDev od[3] = {};
+        uint32_t has = 0;
+        for (int i = 0; i < 3; i++)
+            if (outs[i]) {
+                od[i] = out_dev(outs[i]);
+                has |= 1u << i;
+            }
+        e = cudaFuncSetAttribute(gb_extract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGbExtractSmem);
+        if (e != cudaSuccess) return cuda_fail(e, "groupby: extraction shared memory attribute");
+        gb_extract_kernel<<<1, kGbExtractThreads, kGbExtractSmem, s>>>(
+            reinterpret_cast<const unsigned long long*>(w + L.sums), reinterpret_cast<const unsigned long long*>(w + L.counts),
+            (uint32_t)g, od[0], od[1], od[2], has, d_groups);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: extraction launch");
+        return AMX_OK;
+    }
     iota_kernel<<<(unsigned)((g + 255) / 256 < 4096 ? (g + 255) / 256 : 4096), 256, 0, s>>>(
         reinterpret_cast<uint32_t*>(w + L.iota), g);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: iota launch");
