@@ -264,3 +264,42 @@ def test_repeated_calls_reuse_workspace(cuda):
         assert int(cnt[0].item()) == wcnt
         assert np.array_equal(gpu_bytes(out, wcnt), want)
     ops.workspace_status(ws)
+
+
+def plain_pair_cases():
+    from amethyst_b200 import _capi as A
+
+    ops8 = [A.OP_ADD, A.OP_SUB, A.OP_MUL, A.OP_MIN, A.OP_MAX, A.OP_AND, A.OP_OR, A.OP_XOR]
+    out = []
+    for lb, rb in [(7, 13), (13, 7), (11, 11), (13, 13)]:
+        for op in ops8:
+            out.append((op, lb, rb))
+    return out
+
+
+@pytest.mark.parametrize("op,lb,rb", plain_pair_cases())
+def test_chain_plain_pair_kernels(cuda, op, lb, rb):
+    """Compacting chains with no mask out and a sum or nothing (the plain two-column kernels, one
+    per slab-width pair and op) and with another aggregate (the general kernel), into slabs of
+    the op's natural width (compile-time encoder), other slab widths, plain32 and nogaps."""
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    vb = int(A.lib().amx_binary_out_bits(op, lb, rb))
+    for n in (200003, 1 << 20):
+        lv, lraw = make_column(lb * 13 + op + n, SLAB, lb, n)
+        rv, rraw = make_column(rb * 29 + op + n, SLAB, rb, n)
+        lc, rc = to_gpu(lraw, n, SLAB, lb), to_gpu(rraw, n, SLAB, rb)
+        top = (1 << vb) - 1
+        for pk, k0 in [(A.PRED_LT, top // 3 + 1), (A.PRED_GE, top // 2)]:
+            p = ops.predicate(pk, k0, 0, vb)
+            for agg, want_agg in [(A.AGG_SUM, True), (A.AGG_SUM, False), (A.AGG_MAX, True)]:
+                for of, ob in [(SLAB, vb), (SLAB, 16), (PLAIN32, 32), (NOGAPS, vb)]:
+                    out, _, cnt, ag = ops.chain(lc, rc, op, vb, p, agg, out_fmt=of, out_bits=ob, want_agg=want_agg)
+                    wout, wcnt, wagg = O.chain(op, (lraw, SLAB, lb), (rraw, SLAB, rb), vb, O.pred(pk, k0, 0, vb), agg,
+                                               of, ob, n)
+                    c = int(cnt[0].item())
+                    assert c == wcnt, (op, lb, rb, n, pk, agg, of, ob)
+                    if want_agg:
+                        assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (op, lb, rb, n, pk, agg)
+                    assert np.array_equal(gpu_bytes(out, c), wout), (op, lb, rb, n, pk, agg, of, ob)
