@@ -88,7 +88,8 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
         swar_setup(p);
         return launch_swar((uint32_t)(id - kSwarPolicyBase), p, ws, ws_bytes, stream);
     }
-    if (plain_compacting(p)) {  // the two-column policies' variants that carry only this path
+    if (plain_compacting(p)) {  // the variants that carry only this path
+        if (id == 0) return launch<GenericPolT<12, true>>(p, ws, ws_bytes, stream);
         switch (id) {
 #define AMX_PLAIN_CASE(id, a, b) case id:
             AMX_SLAB2_PAIRS(AMX_PLAIN_CASE)

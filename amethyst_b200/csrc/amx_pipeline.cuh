@@ -1059,15 +1059,19 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
     }
 }
 
-// Any formats and widths: warp-major runtime readers, 64-bit values, 16 elements per thread.
-struct GenericPol {
+// Any formats and widths: warp-major runtime readers, 64-bit values, RR elements per thread.
+// PLAIN: the variant for compacting requests with 16-bit values, no masks and at most a sum
+// (the request's path only, and twice the elements per thread to halve the tiles).
+template <int RR = 8, bool PLAIN = false>
+struct GenericPolT {
     using V = uint64_t;
-    static constexpr int R = 8;
+    static constexpr int R = RR;
     static constexpr bool kWarpMajor = true;
     static constexpr bool kSwar = false;
-    static constexpr bool kPlain = false;
+    static constexpr bool kPlain = PLAIN;
     static constexpr bool kFilter = false;
     static constexpr bool kAggOnly = false;
+    static constexpr int kOutBits = 0;         // the encoder warps use the runtime encoder
     static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;
 
@@ -1106,5 +1110,6 @@ struct GenericPol {
         return 0;
     }
 };
+using GenericPol = GenericPolT<>;
 
 }  // namespace amx

@@ -303,3 +303,32 @@ def test_chain_plain_pair_kernels(cuda, op, lb, rb):
                     if want_agg:
                         assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (op, lb, rb, n, pk, agg)
                     assert np.array_equal(gpu_bytes(out, c), wout), (op, lb, rb, n, pk, agg, of, ob)
+
+
+@pytest.mark.parametrize("lf,lb,rf,rb,op", [
+    (PLAIN32, 7, PLAIN32, 13, 0), (PLAIN32, 12, NOGAPS, 9, 1), (NOGAPS, 5, PLAIN64, 11, 9),
+    (PLAIN64, 14, SLAB, 14, 6), (SLAB, 6, SLAB, 9, 2), (PLAIN32, 16, PLAIN32, 16, 5)])
+def test_chain_plain_generic_kernel(cuda, lf, lb, rf, rb, op):
+    """Compacting chains outside the compile-time width pairs, with no mask out and a sum or
+    nothing (the plain variant of the runtime-format policy) or another aggregate (the general
+    one), against the oracle."""
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    vb = int(A.lib().amx_binary_out_bits(op, lb, rb))
+    for n in (1, 6143, 6145, 300007):
+        lv, lraw = make_column(lb * 7 + op + n, lf, lb, n)
+        rv, rraw = make_column(rb * 5 + op + n, rf, rb, n)
+        lc, rc = to_gpu(lraw, n, lf, lb), to_gpu(rraw, n, rf, rb)
+        top = (1 << vb) - 1
+        p = ops.predicate(A.PRED_BETWEEN, top // 5, top // 2, vb)
+        for agg, want_agg in [(A.AGG_SUM, True), (A.AGG_SUM, False), (A.AGG_XOR, True)]:
+            for of, ob in [(SLAB, vb), (PLAIN32, 32), (NOGAPS, vb)]:
+                out, _, cnt, ag = ops.chain(lc, rc, op, vb, p, agg, out_fmt=of, out_bits=ob, want_agg=want_agg)
+                wout, wcnt, wagg = O.chain(op, (lraw, lf, lb), (rraw, rf, rb), vb,
+                                           O.pred(A.PRED_BETWEEN, top // 5, top // 2, vb), agg, of, ob, n)
+                c = int(cnt[0].item())
+                assert c == wcnt, (lf, lb, rf, rb, op, n, agg, of)
+                if want_agg:
+                    assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (lf, lb, rf, rb, op, n, agg)
+                assert np.array_equal(gpu_bytes(out, c), wout), (lf, lb, rf, rb, op, n, agg, of)
