@@ -88,6 +88,14 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
         swar_setup(p);
         return launch_swar((uint32_t)(id - kSwarPolicyBase), p, ws, ws_bytes, stream);
     }
+    // element-wise output with nothing else (conversions, binary ops): the runtime-format map
+    // variant, where its larger tiles still leave room for two stages and the output slot
+    if (id == 0 && p.has_out && !p.compact && !p.has_mask_in && !p.mask_out && !p.has_agg) {
+        constexpr uint32_t kT = 512 * 12;
+        const uint64_t stage = stage_need(p.a, kT) + (p.has_b ? stage_need(p.b, kT) : 0);
+        const uint64_t slot = round_up(kT * (p.vbits <= 16 ? 2u : 8u), 128);
+        if (kCvOff + slot + 2 * stage <= 220 * 1024) return launch<GenericPolT<12, false, true>>(p, ws, ws_bytes, stream);
+    }
     if (plain_compacting(p)) {  // the variants that carry only this path
         if (id == 0) return launch<GenericPolT<12, true>>(p, ws, ws_bytes, stream);
         switch (id) {

@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         uint64_t fl;
         Pol::decode(p, st, sbase + 3 * s, e0, v, fl);
         // element of flag bit i: thread-contiguous tid*R + i, warp-major warp*32R + 32i + lane
-        if (!Pol::kPlain && p.has_mask_in) {
+        if (!Pol::kPlain && !Pol::kMap && p.has_mask_in) {
             const uint32_t* mw = reinterpret_cast<const uint32_t*>(st + p.m_off);
             if (WM) {
                 uint64_t mfl = 0;
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             for (int i = 0; i < R; i++) a += ((fl >> i) & 1) ? (uint64_t)v[i] : 0;
             my_agg += a;
         }
-        else if (!Pol::kPlain && p.has_agg && !sparse) {
+        else if (!Pol::kPlain && !Pol::kMap && p.has_agg && !sparse) {
             uint64_t a = 0;
             switch (p.agg) {
                 case AMX_AGG_SUM:
@@ -813,7 +813,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 bal[i] = __ballot_sync(0xffffffffu, (fl >> i) & 1);
                 c += __popc(bal[i]);
             }
-            if (!Pol::kPlain && p.mask_out) {
+            if (!Pol::kPlain && !Pol::kMap && p.mask_out) {
                 uint32_t word = 0;
 #pragma unroll
                 for (int i = 0; i < R; i++)
@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         }
         else {
             c = __popcll(fl);
-            if (!Pol::kPlain && p.mask_out && fl) {
+            if (!Pol::kPlain && !Pol::kMap && p.mask_out && fl) {
                 const uint32_t le0 = tid * R;
                 const uint32_t wi = le0 >> 5, sh = le0 & 31;
                 atomicOr(&bitmap[wi], (uint32_t)(fl << sh));
@@ -834,7 +834,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         }
         my_count += WM ? (lane == 0 ? c : 0) : c;
 
-        if (Pol::kPlain || p.has_out) {
+        if (Pol::kPlain || Pol::kMap || p.has_out) {
             // block scan: survivors before this thread (or warp) inside the tile
             volatile uint32_t* wt = warp_tot + 32 * (j & 1);
             uint32_t pos, total = 0, before = 0;
@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 pos = before + incl - c;
             }
             uint8_t* slot = cv;
-            if (Pol::kPlain || compact) {
+            if (Pol::kPlain || (!Pol::kMap && compact)) {
                 // publish this tile's survivor count for the other CTAs' look-backs at once ...
                 if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
                 // ... but reuse slot q only after the encoder warps are done with its last tile
@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 for (int i = 0; i < R; i++)
                     if ((fl >> i) & 1) *dst++ = v[i];
             }
-            if (Pol::kPlain || compact) {
+            if (Pol::kPlain || (!Pol::kMap && compact)) {
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&scat[q]);  // this warp's survivors are in slot q
                 if (++q == NB) {
@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             }
         }
         if (!WM) {
-            if (!Pol::kPlain && !p.has_out && p.has_agg && sparse) {
+            if (!Pol::kPlain && !Pol::kMap && !p.has_out && p.has_agg && sparse) {
                 uint64_t a = 0;
                 for (uint64_t f = fl; f; f &= f - 1) {
                     const V x = Pol::value_at(p, st, sbase + 3 * s, e0, __ffsll((long long)f) - 1);
@@ -934,7 +934,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);  // this warp is done with stage s
         }
-        if (!Pol::kPlain && !WM && p.mask_out) {
+        if (!Pol::kPlain && !Pol::kMap && !WM && p.mask_out) {
             compute_bar();
             const uint32_t words = (valid + 31) / 32;
             for (uint32_t i = tid; i < words; i += T) {
@@ -1060,9 +1060,10 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
 }
 
 // Any formats and widths: warp-major runtime readers, 64-bit values, RR elements per thread.
-// PLAIN: the variant for compacting requests with 16-bit values, no masks and at most a sum
-// (the request's path only, and twice the elements per thread to halve the tiles).
-template <int RR = 8, bool PLAIN = false>
+// PLAIN: the variant for compacting requests with 16-bit values, no masks and at most a sum;
+// MAP: for element-wise outputs (conversions, binary ops) with no masks and no aggregate.  Both
+// carry their request's path only, with more elements per thread to cut the tiles.
+template <int RR = 8, bool PLAIN = false, bool MAP = false>
 struct GenericPolT {
     using V = uint64_t;
     static constexpr int R = RR;
@@ -1071,6 +1072,7 @@ struct GenericPolT {
     static constexpr bool kPlain = PLAIN;
     static constexpr bool kFilter = false;
     static constexpr bool kAggOnly = false;
+    static constexpr bool kMap = MAP;
     static constexpr int kOutBits = 0;         // the encoder warps use the runtime encoder
     static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;

@@ -89,6 +89,7 @@ struct SwarPol {
     static constexpr bool kPlain = PLAIN;
     static constexpr bool kFilter = FILTER;    // the request only writes the bitmask
     static constexpr bool kAggOnly = AGGONLY;  // the request only counts and aggregates
+    static constexpr bool kMap = false;
     // the plain compressstore at widths of at most 5 fields per slab runs 24 compute warps (its
     // registers allow 960 threads): more warps to hide the compute warps' latencies
     static constexpr uint32_t kCompute = ((PLAIN || FILTER || AGGONLY) && EPS * SPT <= 40) ? 768 : 512;
