@@ -13,7 +13,7 @@ maps 16 features of the decision point to one of the four candidates.
 
   sweep_labels(chain)  times every candidate of every decision point (the operator plus its
                        consumer, CUDA events) and labels it with the fastest -- the training data;
-  exhaustive(chain)    times every combination of candidates for a whole chain: the judge of the
+  exhaustive(chain)    times every combination of candidates for a whole chain: the yardstick for the
                        selector's regret and its fallback;
   Selector             the trained network; `decide` falls back to timing the candidates on the
                        spot when its top probability is below `confidence`.
