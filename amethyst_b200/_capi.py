@@ -53,6 +53,18 @@ class BatchPlan(C.Structure):
                 ("items", C.c_uint64), ("workspace_bytes", C.c_uint64)]
 
 
+STEP_FILTER, STEP_COMPRESSSTORE, STEP_BINARY, STEP_REDUCE, STEP_GROUPBY = range(5)
+FORMAT_FUSED = 0xFF
+PROGRAM_MAX_STEPS = 32
+
+
+class Step(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("op", C.c_uint32), ("value_bits", C.c_uint32), ("out_format", C.c_uint32),
+                ("out_bits", C.c_uint32), ("reserved", C.c_uint32), ("pred", Predicate), ("aux", Column),
+                ("d_result", C.c_void_p), ("group_keys", Column), ("group_sums", Column),
+                ("group_counts", Column)]
+
+
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libamethyst_b200.so")
 
 _P = C.c_void_p
@@ -68,6 +80,7 @@ _SIGS = {
     "amx_workspace_status": (C.c_int, [_P, _P]),
     "amx_set_tuning": (C.c_int, [C.POINTER(Tuning)]),
     "amx_get_tuning": (C.c_int, [C.POINTER(Tuning)]),
+    "amx_test_lookback_timeout": (C.c_int, [C.c_uint64, C.c_uint32]),
     "amx_filter": (C.c_int, [_COL, C.POINTER(Predicate), _P, _P, C.c_size_t, _P]),
     "amx_compressstore": (C.c_int, [_COL, _P, _COL, _P, _P, C.c_size_t, _P]),
     "amx_filter_compressstore": (C.c_int, [_COL, C.POINTER(Predicate), _COL, _P, _P, C.c_size_t, _P]),
@@ -90,6 +103,17 @@ _SIGS = {
     "amx_mlp_param_count": (C.c_uint32, [C.c_uint32]),
     "amx_mlp_forward": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P]),
     "amx_mlp_train_step": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, C.c_float, _P, _P]),
+    "amx_program_create": (C.c_int, [_COL, C.POINTER(Step), C.c_uint32, C.POINTER(C.c_void_p)]),
+    "amx_program_workspace_bytes": (C.c_uint64, [_P]),
+    "amx_program_run": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "amx_program_output": (C.c_int, [_P, _P, _COL, C.POINTER(C.c_void_p)]),
+    "amx_program_status": (C.c_int, [_P, _P, _P]),
+    "amx_program_destroy": (None, [_P]),
+    "amx_graph_capture": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_uint64), C.c_uint32,
+                                    C.c_uint32, C.POINTER(C.c_void_p)]),
+    "amx_graph_launch": (C.c_int, [_P, _P]),
+    "amx_graph_destroy": (None, [_P]),
+    "amx_bit_histogram": (C.c_int, [_COL, _P, _P]),
     "amx_fill_uniform": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, _P]),
     "amx_fill_from_cdf": (C.c_int, [_P, C.c_uint64, _P, C.c_uint32, C.c_uint64, _P]),
 }

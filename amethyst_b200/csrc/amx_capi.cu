@@ -217,6 +217,14 @@ amx_status amx_set_tuning(const amx_tuning* t)
     return AMX_OK;
 }
 
+amx_status amx_test_lookback_timeout(uint64_t tile, uint32_t wait_polls)
+{
+    LookbackFault& f = lookback_fault();
+    f.withhold_plus1 = tile == ~0ull ? 0 : tile + 1;
+    f.wait_polls = tile == ~0ull ? 0 : wait_polls;
+    return AMX_OK;
+}
+
 amx_status amx_get_tuning(amx_tuning* t)
 {
     if (!t) return fail(AMX_ERR_INVALID_ARG, "get_tuning: null output");

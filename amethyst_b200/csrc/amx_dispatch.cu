@@ -15,11 +15,20 @@ amx_tuning& tuning()
     return t;
 }
 
+LookbackFault& lookback_fault()
+{
+    static thread_local LookbackFault f{};
+    return f;
+}
+
 amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t stream)
 {
     PipeParams p{};
+    p.withhold_plus1 = lookback_fault().withhold_plus1;
+    p.wait_polls = lookback_fault().wait_polls ? lookback_fault().wait_polls : kWaitSpins;
     p.a = col_dev(r.a);
     p.n = r.a->n;
+    p.n_dev = r.n_dev;
     if (r.b) {
         p.b = col_dev(r.b);
         p.has_b = 1;

@@ -28,10 +28,18 @@ struct ChainReq {
     uint32_t agg = AMX_AGG_SUM;
     uint64_t* agg_out = nullptr;
     int force_policy = -1;  // -1 = automatic; otherwise a policy id (tests and the autotuner)
+    const uint64_t* n_dev = nullptr;  // device-resident length (<= a->n), read by the kernel
 };
 
 // launch tuning of this host thread (amx_set_tuning); zero fields mean "automatic"
 amx_tuning& tuning();
+
+// look-back fault injection of this host thread (amx_test_lookback_timeout)
+struct LookbackFault {
+    uint64_t withhold_plus1 = 0;  // tile + 1 whose count the kernel never publishes, 0: none
+    uint32_t wait_polls = 0;      // 0: kWaitSpins
+};
+LookbackFault& lookback_fault();
 
 amx_status fail(amx_status s, const char* fmt, ...);
 amx_status cuda_fail(cudaError_t e, const char* what);
@@ -46,6 +54,14 @@ amx_status normalize_pred(const amx_predicate* p, uint64_t& lo, uint64_t& span, 
 int sm_count();
 
 amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t stream);
+
+// amx_groupby with an optional device-resident length of the key and value columns (<= keys->n)
+amx_status groupby_run(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                       const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                       uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream, const uint64_t* n_dev);
+// offset of the tile-pipeline workspace inside a group-by workspace when the groups of keys of
+// that width are extracted by the pipeline, else UINT64_MAX
+uint64_t groupby_pipeline_offset(uint32_t key_bits);
 
 // plain compacting two-column policy `id` (amx_pairs.cu): one kernel per pair and cheap op
 amx_status launch_plain_pair(int id, PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t stream);

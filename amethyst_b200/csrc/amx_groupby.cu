@@ -48,7 +48,16 @@ struct GbParams {
     uint32_t pad;          // alignment of the pointers below
     unsigned long long* gsum;
     unsigned long long* gcnt;
+    const uint64_t* n_dev;  // optional device-resident length (<= n), read by the kernels
 };
+
+// elements of this run: n, or the device-resident length a previous kernel wrote
+__device__ __forceinline__ uint64_t gb_len(const GbParams& p)
+{
+    if (!p.n_dev) return p.n;
+    const uint64_t d = *p.n_dev;
+    return d < p.n ? d : p.n;
+}
 
 // element e of column c read straight from global memory (consecutive lanes share words)
 __device__ __forceinline__ uint64_t load_elem(const ColDev& c, uint64_t e)
@@ -212,7 +221,8 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
     uint32_t* thi = tab + 2 * slots;   // carries out of the low word (unused when NOCARRY)
     uint32_t* tcnt = tab + 3 * slots;  // count
     const uint32_t tid = threadIdx.x;
-    const uint64_t nchunks = (p.n + kGbChunk - 1) / kGbChunk;
+    const uint64_t n = gb_len(p);
+    const uint64_t nchunks = (n + kGbChunk - 1) / kGbChunk;
     const uint64_t flush_every = p.flush_every;
 
     auto clear = [&]() {
@@ -226,7 +236,7 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
     uint64_t seen = 0;
     for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const uint64_t e0 = chunk * kGbChunk;
-        const uint64_t e1 = e0 + kGbChunk < p.n ? e0 + kGbChunk : p.n;
+        const uint64_t e1 = e0 + kGbChunk < n ? e0 + kGbChunk : n;
         // each thread walks a run of kGbRun consecutive elements of the chunk; a run starts on
         // a multiple of 32, so its mask bits are one mask word
         const uint64_t r0 = e0 + (uint64_t)tid * kGbRun;
@@ -336,7 +346,8 @@ __global__ void __launch_bounds__(kGbThreads) groupby_phase_kernel(const __grid_
     const uint32_t tid = threadIdx.x;
     const uint32_t run = p.run;
     const uint64_t chunk_elems = (uint64_t)kGbThreads * run;
-    const uint64_t nchunks = (p.n + chunk_elems - 1) / chunk_elems;
+    const uint64_t n = gb_len(p);
+    const uint64_t nchunks = (n + chunk_elems - 1) / chunk_elems;
 
     for (uint32_t i = tid; i < slots; i += blockDim.x) {
         if (!DENSE) tkey[i] = kEmptyKey;
@@ -346,7 +357,7 @@ __global__ void __launch_bounds__(kGbThreads) groupby_phase_kernel(const __grid_
     uint64_t seen = 0;
     for (uint64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
         const uint64_t e0 = chunk * chunk_elems;
-        const uint64_t e1 = e0 + chunk_elems < p.n ? e0 + chunk_elems : p.n;
+        const uint64_t e1 = e0 + chunk_elems < n ? e0 + chunk_elems : n;
         const uint64_t r0 = e0 + (uint64_t)tid * run;
         const uint32_t rn = r0 >= e1 ? 0 : (uint32_t)(e1 - r0 < run ? e1 - r0 : run);
         if (rn) {
@@ -404,7 +415,8 @@ static uint32_t gcd_u32(uint32_t a, uint32_t b) { return b ? gcd_u32(b, a % b) :
 __global__ void groupby_wide_kernel(const __grid_constant__ GbParams p)
 {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < p.n; e += stride) {
+    const uint64_t n = gb_len(p);
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
         if (p.mask && !((__ldg(p.mask + (e >> 5)) >> (e & 31)) & 1u)) continue;
         const uint32_t key = (uint32_t)load_elem(p.k, e);
         atomicAdd(&p.gsum[key], (unsigned long long)load_elem(p.v, e));
@@ -512,6 +524,12 @@ static GbLayout gb_layout(uint32_t kbits)
     return l;
 }
 
+uint64_t groupby_pipeline_offset(uint32_t key_bits)
+{
+    if (key_bits < 1 || key_bits > kGbMaxKeyBits || (1ull << key_bits) <= kGbExtractMax) return ~0ull;
+    return gb_layout(key_bits).ws;
+}
+
 }  // namespace amx
 
 using namespace amx;
@@ -527,6 +545,17 @@ uint64_t amx_groupby_workspace_bytes(uint32_t key_bits)
 amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
                        const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
                        uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream)
+{
+    return groupby_run(keys, vals, d_mask, out_keys, out_sums, out_counts, d_groups, ws, ws_bytes, stream, nullptr);
+}
+
+}  // extern "C"
+
+namespace amx {
+
+amx_status groupby_run(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                       const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                       uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream, const uint64_t* n_dev)
 {
     amx_status st = check_column(keys, "groupby: keys");
     if (st) return st;
@@ -562,6 +591,7 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
     p.dense = keys->bits <= kGbDenseBits;
     p.gsum = reinterpret_cast<unsigned long long*>(w + L.sums);
     p.gcnt = reinterpret_cast<unsigned long long*>(w + L.counts);
+    p.n_dev = n_dev;
     if (p.n) {
         if (vals->bits <= 32) {
             const bool nocarry = vals->bits <= kGbNoCarryBits;
@@ -646,4 +676,4 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
     return AMX_OK;
 }
 
-}  // extern "C"
+}  // namespace amx

@@ -8,8 +8,9 @@
 
 namespace amx {
 
-// Upper bound of every device-side spin (mbarrier phases, look-back flags).  Each spin
-// backs off with __nanosleep, so the bound is well above a second of waiting.
+// Upper bound of the polls of one look-back status word (each poll after the eighth backs off
+// with __nanosleep): well above a second of waiting.  mbarrier waits have their own bound
+// (amx_device.cuh: kWaitSuspends suspensions of kWaitSuspendNs).
 constexpr uint32_t kWaitSpins = 1u << 20;
 
 // A column as the kernels see it.
@@ -81,8 +82,9 @@ struct PipeParams {
     uint64_t* agg_out;
     WsHeader* ws;
     uint64_t* status;
-    uint64_t n;
-    uint64_t num_tiles;
+    uint64_t n;            // elements (the capacity when n_dev is set)
+    uint64_t num_tiles;    // tiles of n elements
+    const uint64_t* n_dev; // optional device-resident length: the kernel runs min(n, *n_dev) elements
     uint32_t tile_elems;
     uint32_t stage_bytes;  // bytes of one pipeline stage (a | b | m buffers)
     uint32_t stages;       // stages in the ring, 2..kMaxStages
@@ -98,7 +100,8 @@ struct PipeParams {
     // form the interval [lo, hi1) or its complement; sw_l1 / sw_l2 are lo and hi1 repeated in
     // every field with the field's top bit cleared, sw_h has the top bit of every field set
     uint32_t sw_mode;  // kSw* bits
-    uint32_t sw_pad;
+    uint32_t wait_polls;      // polls of a look-back status word before giving up (kWaitSpins)
+    uint64_t withhold_plus1;  // test hook: tile + 1 whose count is never published (0: none)
     uint64_t sw_h;
     uint64_t sw_l1;
     uint64_t sw_l2;

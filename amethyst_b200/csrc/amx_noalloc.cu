@@ -16,7 +16,12 @@
 //     uses (cudaMemsetAsync) before its kernel runs, so calls that follow one another on a stream
 //     are safe, but calls that may overlap on the GPU (other streams, other host threads) race;
 //   * the first call on a device looks up the array's device address there (cudaGetSymbolAddress)
-//     and caches it; make that first call before any stream capture begins.
+//     and caches it; make that first call before any stream capture begins.  The cached address
+//     belongs to the device's primary context: after cudaDeviceReset it is stale, so a process
+//     that resets a device must not call this entry point on that device again;
+//   * a device-side failure (a bounded wait that ran out) is recorded in the array's header;
+//     amx_filter_compressstore_noalloc_status() reads it back.  The next call clears it, so check
+//     it before the next call.
 // No cudaMalloc, cudaFree or allocating library routine is called on this path.
 #include <mutex>
 
@@ -81,4 +86,18 @@ extern "C" amx_status amx_filter_compressstore_noalloc(const amx_column* in, con
     r.compact = 1;
     r.count_out = d_count;
     return run_chain(r, scratch, kNoAllocScratchBytes, (cudaStream_t)stream);
+}
+
+extern "C" amx_status amx_filter_compressstore_noalloc_status(void* stream)
+{
+    void* scratch = nullptr;
+    amx_status st = scratch_for_current_device(&scratch);
+    if (st) return st;
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "filter_compressstore_noalloc_status: stream");
+    uint32_t err = 0;
+    e = cudaMemcpy(&err, &static_cast<const WsHeader*>(scratch)->err, sizeof(err), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "filter_compressstore_noalloc_status: read");
+    if (err) return fail((amx_status)err, "device-side failure recorded by the last no-alloc call (%u)", err);
+    return AMX_OK;
 }

@@ -66,11 +66,11 @@ __device__ __forceinline__ void tile_bytes(const ColDev& c, uint64_t stride, uin
 // Issue the staging of one tile into stage buffer `st` (one thread): plain scalar code, no
 // arrays, so the loader spends as little time as possible per tile.
 __device__ __forceinline__ void stage_issue(const PipeParams& p, uint8_t* st, uint64_t* sbase, uint64_t* bar,
-                                            uint64_t tile, uint32_t tile_elems)
+                                            uint64_t tile, uint32_t tile_elems, uint64_t n)
 {
     const uint64_t e0 = tile * tile_elems;
     uint64_t e1 = e0 + tile_elems;
-    if (e1 > p.n) e1 = p.n;
+    if (e1 > n) e1 = n;
     uint64_t a0, a1, b0 = 0, b1 = 0, m0 = 0, m1 = 0;
     tile_bytes(p.a, p.a_stride, tile, e0, e1, a0, a1);
     if (p.has_b) tile_bytes(p.b, p.b_stride, tile, e0, e1, b0, b1);
@@ -274,7 +274,8 @@ __device__ __forceinline__ void encode_slab_ct(const OutDev& o, const V* cv, uin
 // are bounded: on timeout the error word is set and the count is taken as 0.
 constexpr int kLookPerLane = 8;
 
-__device__ __forceinline__ uint64_t sum_counts(const uint64_t* status, uint64_t lo, uint64_t hi, uint32_t* err)
+__device__ __forceinline__ uint64_t sum_counts(const uint64_t* status, uint64_t lo, uint64_t hi, uint32_t* err,
+                                               uint32_t limit)
 {
     const uint32_t lane = threadIdx.x & 31;
     uint64_t acc = 0;
@@ -290,7 +291,7 @@ __device__ __forceinline__ uint64_t sum_counts(const uint64_t* status, uint64_t 
             const uint64_t idx = base + lane + 32 * m;
             uint32_t spins = 0;
             while ((st[m] >> 62) == 0) {  // that tile is still being decoded
-                if (++spins > kWaitSpins) {
+                if (++spins > limit) {
                     record_error(err, AMX_ERR_TIMEOUT);
                     st[m] = kFlagAgg;
                     break;
@@ -346,7 +347,7 @@ __device__ __forceinline__ void wait_or_flag(uint64_t* bar, uint32_t parity, uin
 //   [224,256) cvfree[4]                                                        (mbarriers)
 //   [256,320)  tickets[8]              [320,512) stage base offsets [8][3]
 //   [512,768)  warp totals [2][32]     [768,1024) warp counts [32]  [1024,1280) warp aggregates [32]
-//   [1280,1360) per-slot tile / total / offset                     [1536,5632) tile bitmap (thread-contiguous policies)
+//   [1280,1360) per-slot tile / total / offset  [1360,1376) run length, tiles                    [1536,5632) tile bitmap (thread-contiguous policies)
 //   [kCvOff, smem_fixed)  gathered-value slots;  [smem_fixed, ...) p.stages stage buffers
 constexpr uint32_t kBitmapOff = 1536;
 constexpr uint32_t kCvOff = 5632;
@@ -405,6 +406,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     volatile uint64_t* slot_tile = reinterpret_cast<volatile uint64_t*>(smem + 1280);
     volatile uint32_t* slot_total = reinterpret_cast<volatile uint32_t*>(smem + 1312);
     volatile uint64_t* slot_g = reinterpret_cast<volatile uint64_t*>(smem + 1328);
+    uint64_t* run_len = reinterpret_cast<uint64_t*>(smem + 1360);
     uint32_t* bitmap = reinterpret_cast<uint32_t*>(smem + kBitmapOff);
     uint8_t* cv = smem + kCvOff;
     uint8_t* stage0 = smem + p.smem_fixed;
@@ -427,10 +429,20 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             mbar_init(&cvfree[q], kEncoderWarps);
         }
         fence_mbar_init();
+        // elements of this run: the capacity, or the device-resident length a previous kernel
+        // on the stream wrote (a count that never reached the host)
+        uint64_t len = p.n;
+        if (p.n_dev) {
+            const uint64_t d = *p.n_dev;
+            if (d < len) len = d;
+        }
+        run_len[0] = len;
+        run_len[1] = (len + TILE - 1) / TILE;
     }
     if (!WM)
         for (uint32_t i = tid; i < TILE / 32; i += blockDim.x) bitmap[i] = 0;
     __syncthreads();  // the last CTA-wide barrier: roles split below
+    const uint64_t n = run_len[0], num_tiles = run_len[1];
 
     // ---------------------------------------------------------------- loader warp
     if (warp == NW) {
@@ -440,25 +452,25 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             // there, so they release no stage from that iteration on.
             uint64_t stop_at = kNoTile;
             for (uint32_t s = 0; s < S; s++) {
-                const uint64_t tk = stop_at == kNoTile ? atomicAdd(&p.ws->ticket, 1u) : p.num_tiles;
+                const uint64_t tk = stop_at == kNoTile ? atomicAdd(&p.ws->ticket, 1u) : num_tiles;
                 tickets[s] = tk;
-                if (tk < p.num_tiles)
-                    stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &full[s], tk, TILE);
+                if (tk < num_tiles)
+                    stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &full[s], tk, TILE, n);
                 else {
                     mbar_arrive(&full[s]);
                     if (stop_at == kNoTile) stop_at = s;
                 }
             }
             // the next ticket is taken one refill ahead, so its atomic latency overlaps the wait
-            uint64_t next = stop_at == kNoTile ? atomicAdd(&p.ws->ticket, 1u) : p.num_tiles;
+            uint64_t next = stop_at == kNoTile ? atomicAdd(&p.ws->ticket, 1u) : num_tiles;
             uint32_t s = 0, phase = 0;
             for (uint64_t j = 0; j < stop_at; j++) {
                 wait_or_flag(&empty[s], phase, &p.ws->err);  // iteration j released stage s
-                const uint64_t tk = stop_at == kNoTile ? next : p.num_tiles;
-                if (tk < p.num_tiles) next = atomicAdd(&p.ws->ticket, 1u);
+                const uint64_t tk = stop_at == kNoTile ? next : num_tiles;
+                if (tk < num_tiles) next = atomicAdd(&p.ws->ticket, 1u);
                 tickets[s] = tk;  // for iteration j + S
-                if (tk < p.num_tiles)
-                    stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &full[s], tk, TILE);
+                if (tk < num_tiles)
+                    stage_issue(p, stage0 + s * p.stage_bytes, sbase + 3 * s, &full[s], tk, TILE, n);
                 else {
                     mbar_arrive(&full[s]);
                     if (stop_at == kNoTile) stop_at = j + S;
@@ -485,7 +497,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 const uint64_t tile = slot_tile[q];
                 if (tile != kNoTile) {
                     const uint64_t lo = first ? 0 : prev_tile + 1;
-                    const uint64_t g = (first ? 0 : prev_end) + sum_counts(p.status, lo, tile, &p.ws->err);
+                    const uint64_t g = (first ? 0 : prev_end) + sum_counts(p.status, lo, tile, &p.ws->err, p.wait_polls);
                     first = false;
                     prev_tile = tile;
                     prev_end = g + slot_total[q];
@@ -520,23 +532,23 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     if (Pol::kPlain || (p.out.format == AMX_SLAB && p.out.bits == (uint32_t)Pol::kBits)) {
                         if (Pol::kPlain || cv16)
                             encode_slab_ct<Pol::kBits, uint16_t>(p.out, reinterpret_cast<const uint16_t*>(sv),
-                                                                slot_total[q], slot_g[q], tile == p.num_tiles - 1,
+                                                                slot_total[q], slot_g[q], tile == num_tiles - 1,
                                                                 etid, 32 * kEncoderWarps);
                         else if constexpr (!Pol::kPlain)
                             encode_slab_ct<Pol::kBits, uint32_t>(p.out, reinterpret_cast<const uint32_t*>(sv),
-                                                                slot_total[q], slot_g[q], tile == p.num_tiles - 1,
+                                                                slot_total[q], slot_g[q], tile == num_tiles - 1,
                                                                 etid, 32 * kEncoderWarps);
                         done = true;
                     }
                 }
                 if constexpr (!Pol::kPlain) {
                     if (!done)
-                        encode_any<V>(p.out, sv, cv16, slot_total[q], slot_g[q], tile == p.num_tiles - 1, etid,
+                        encode_any<V>(p.out, sv, cv16, slot_total[q], slot_g[q], tile == num_tiles - 1, etid,
                                       32 * kEncoderWarps);
                 }
                 else if constexpr (!Pol::kSwar) {
                     const uint16_t* sv16 = reinterpret_cast<const uint16_t*>(sv);
-                    const bool last = tile == p.num_tiles - 1;
+                    const bool last = tile == num_tiles - 1;
                     if constexpr (Pol::kOutBits >= 1 && Pol::kOutBits <= 16) {
                         if (p.out.format == AMX_SLAB && p.out.bits == (uint32_t)Pol::kOutBits)
                             encode_slab_ct<Pol::kOutBits, uint16_t>(p.out, sv16, slot_total[q], slot_g[q], last, etid,
@@ -578,9 +590,9 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             }
             wait_or_flag(&full[s], sphase, &p.ws->err);
             const uint64_t tile = tickets[s];
-            if (tile >= p.num_tiles) break;
+            if (tile >= num_tiles) break;
             const uint64_t e0 = tile * TILE;
-            const uint64_t rem = p.n - e0;
+            const uint64_t rem = n - e0;
             const uint32_t valid = rem < TILE ? (uint32_t)rem : TILE;
             uint64_t x[SPT];
             {
@@ -634,7 +646,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                 uint32_t total, before;
                 tile_prefix<NW>(wt, warp, lane, before, total);
                 pos = before + incl - c;
-                if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
+                if (tid == 0 && tile + 1 != p.withhold_plus1) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
                 if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
                 if (tid == 0) {
                     slot_tile[q] = tile;
@@ -712,10 +724,10 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         }
         wait_or_flag(&full[s], sphase, &p.ws->err);
         const uint64_t tile = tickets[s];
-        if (tile >= p.num_tiles) break;
+        if (tile >= num_tiles) break;
 
         const uint64_t e0 = tile * TILE;
-        const uint64_t rem = p.n - e0;
+        const uint64_t rem = n - e0;
         const uint32_t valid = rem < TILE ? (uint32_t)rem : TILE;
         const uint8_t* st = stage0 + s * p.stage_bytes;
 
@@ -859,7 +871,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             uint8_t* slot = cv;
             if (Pol::kPlain || (!Pol::kMap && compact)) {
                 // publish this tile's survivor count for the other CTAs' look-backs at once ...
-                if (tid == 0) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
+                if (tid == 0 && tile + 1 != p.withhold_plus1) st_relaxed_u64(&p.status[tile], kFlagAgg | total);
                 // ... but reuse slot q only after the encoder warps are done with its last tile
                 if (j >= NB) wait_or_flag(&cvfree[q], qphase ^ 1, &p.ws->err);
                 if (tid == 0) {
@@ -918,7 +930,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             }
             else if constexpr (!Pol::kPlain) {  // element-wise output: the offset is known, encode right away
                 compute_bar();
-                encode_any<V>(p.out, cv, cv16, total, e0, tile == p.num_tiles - 1, tid, T);
+                encode_any<V>(p.out, cv, cv16, total, e0, tile == num_tiles - 1, tid, T);
                 compute_bar();
             }
         }

@@ -229,5 +229,78 @@ class Batch:
         check(lib().amx_batch_status(_ptr(self.ws), _stream_ptr(stream)))
 
 
+def bit_histogram(col: PackedColumn, stream=None) -> torch.Tensor:
+    """65 counters: elements whose value needs exactly k bits (amx_bit_histogram)."""
+    h = torch.zeros(65, dtype=torch.int64, device=col.data.device)
+    check(lib().amx_bit_histogram(C.byref(col.desc), _ptr(h), _stream_ptr(stream)))
+    return h
+
+
+def aligned_bytes(nbytes: int, align: int = 256, device="cuda") -> torch.Tensor:
+    raw = torch.empty(max(nbytes, 1) + align, dtype=torch.uint8, device=device)
+    off = (-raw.data_ptr()) % align
+    return raw[off: off + max(nbytes, 1)]
+
+
+class Program:
+    """An operator-chain program (amx_program_*): the steps run on the device with every
+    intermediate length kept there, so a run can be captured into a CUDA graph.  Holds its
+    workspace and the objects its steps point to."""
+
+    def __init__(self, x: PackedColumn, steps: list, keep: list | None = None, device="cuda"):
+        self.x = x
+        self.keep = keep or []
+        self.nsteps = len(steps)
+        self.steps = (A.Step * max(1, len(steps)))(*steps)
+        h = C.c_void_p()
+        check(lib().amx_program_create(C.byref(x.desc), self.steps, len(steps), C.byref(h)))
+        self.h = h
+        self.ws_bytes = int(lib().amx_program_workspace_bytes(h))
+        self.ws = aligned_bytes(self.ws_bytes, 256, device)
+
+    def run(self, stream=None):
+        check(lib().amx_program_run(self.h, _ptr(self.ws), self.ws_bytes, _stream_ptr(stream)))
+
+    def output(self):
+        """(final column descriptor, device length pointer or None)."""
+        col = A.Column()
+        dl = C.c_void_p()
+        check(lib().amx_program_output(self.h, _ptr(self.ws), C.byref(col), C.byref(dl)))
+        return col, dl.value
+
+    def status(self, stream=None):
+        check(lib().amx_program_status(self.h, _ptr(self.ws), _stream_ptr(stream)))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            lib().amx_program_destroy(h)
+            self.h = None
+
+
+class Graph:
+    """Many programs captured into one CUDA graph (amx_graph_capture), programs spread over
+    `lanes` streams that fork from and join the launching stream."""
+
+    def __init__(self, programs: list, lanes: int = 4):
+        self.programs = programs
+        n = len(programs)
+        hs = (C.c_void_p * max(1, n))(*[p.h.value for p in programs])
+        ws = (C.c_void_p * max(1, n))(*[p.ws.data_ptr() for p in programs])
+        wb = (C.c_uint64 * max(1, n))(*[p.ws_bytes for p in programs])
+        g = C.c_void_p()
+        check(lib().amx_graph_capture(hs, ws, wb, n, lanes, C.byref(g)))
+        self.h = g
+
+    def launch(self, stream=None):
+        check(lib().amx_graph_launch(self.h, _stream_ptr(stream)))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            lib().amx_graph_destroy(h)
+            self.h = None
+
+
 def workspace_status(ws: torch.Tensor, stream=None) -> None:
     check(lib().amx_workspace_status(_ptr(ws), _stream_ptr(stream)))

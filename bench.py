@@ -487,6 +487,108 @@ def groupby_2e28(dev, steps):
     return out
 
 
+def mixed_chain(dev, steps, chains=64, lanes=8, exhaustive=True):
+    """The mixed-chain workload: `chains` held-out synthetic operator chains (2..5 operators from
+    {filter, compressstore, add, sub, mul, sum, min, max, group-by}, n log-uniform in [2^16,
+    2^26], widths 1..32; those with at least one decision point), end to end with the inputs
+    resident in HBM and every scalar result (aggregates, survivor counts, group counts) read back
+    to the host, in two forms:
+      plain     per column and per operator through the single-operator C ABI, every
+                intermediate in slabs at its natural width, survivor counts read back after
+                each compressstore to size the next call;
+      batched   every chain an amx_program with the selector's storage formats, widths and
+                kernel variants, all programs in one CUDA graph over `lanes` streams, one
+                replay and one copy of all results.
+    Regret: each chain's selector pick against the exhaustive best, both timed as replayed
+    graphs of that chain alone.  Every form's results are compared bit for bit."""
+    import numpy as np
+    import torch
+
+    from amethyst_b200 import chains as X
+    from amethyst_b200 import ops
+    from amethyst_b200 import selector as S
+
+    rng = np.random.default_rng(99)
+    specs, k = [], 0
+    while len(specs) < chains:
+        ch = X.random_chain(rng, seed=100000 + k)
+        k += 1
+        if X.decision_points(ch):
+            specs.append(ch)
+    results = torch.zeros(sum(len(c.ops) for c in specs), dtype=torch.int64, device=dev)
+    runners, slot = [], 0
+    for ch in specs:
+        runners.append(S.ChainRunner(ch, results, slot))
+        slot += len(ch.ops)
+    sel = S.Selector.load()
+    picks = sel.choices(runners)
+    progs = [r.program(X.from_combo(p))[0] for r, p in zip(runners, picks)]
+    graph = ops.Graph(progs, lanes=lanes)
+    slab_progs = [r.program(X.fixed(X.DEFAULT_CHOICE))[0] for r in runners]
+    slab_graph = ops.Graph(slab_progs, lanes=lanes)
+    host = torch.empty(results.numel(), dtype=torch.int64, pin_memory=True)
+    stream = torch.cuda.current_stream()
+
+    def plain_step():
+        for r in runners:
+            r.run_plain()
+        host.copy_(results, non_blocking=True)
+        stream.synchronize()
+
+    def graph_step(g):
+        g.launch(stream)
+        host.copy_(results, non_blocking=True)
+        stream.synchronize()
+
+    # bit-exactness: the plain form, the batched selector graph, the fixed-slab graph
+    def digests(final_of):
+        return [r.digest(final_of(i)) for i, r in enumerate(runners)]
+
+    results.zero_()
+    finals = [r.run_plain() for r in runners]
+    torch.cuda.synchronize()
+    ref = digests(lambda i: runners[i].plain_final_column(finals[i]))
+    results.zero_()
+    graph_step(graph)
+    exact = digests(lambda i: runners[i].final_column(progs[i])) == ref
+    results.zero_()
+    graph_step(slab_graph)
+    exact_slab = digests(lambda i: runners[i].final_column(slab_progs[i])) == ref
+
+    reps = max(3, min(steps, 10))
+    timings = {}
+    for name, fn in [("plain", plain_step), ("batched", lambda: graph_step(graph)),
+                     ("batched_fixed_slab", lambda: graph_step(slab_graph))]:
+        for _ in range(2):
+            fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        timings[name] = statistics.median(ts)
+    res = {"workload": f"{len(specs)} held-out operator chains (2-5 operators, n log-uniform [2^16, 2^26], "
+                       "widths 1..32), inputs resident, scalar results to the host",
+           "chains": len(specs), "elements": int(sum(c.n for c in specs)), "lanes": lanes,
+           "plain_ms": round(timings["plain"], 3), "batched_ms": round(timings["batched"], 3),
+           "batched_fixed_slab_ms": round(timings["batched_fixed_slab"], 3),
+           "speedup_e2e": round(timings["plain"] / timings["batched"], 3),
+           "speedup_selector_in_graph": round(timings["batched_fixed_slab"] / timings["batched"], 3),
+           "all_exact": bool(exact and exact_slab), "picks_histogram": np.bincount(
+               [c for p in picks for c in p], minlength=X.K).tolist()}
+    if exhaustive:
+        regrets, combos = [], 0
+        for r, p in zip(runners, picks):
+            best, bc, table = S.exhaustive(r.chain, r, reps=3)
+            combos += len(table)
+            regrets.append(table[tuple(p)] / best - 1.0)
+        res["regret"] = {"median": round(float(np.median(regrets)), 4), "mean": round(float(np.mean(regrets)), 4),
+                         "p90": round(float(np.percentile(regrets, 90)), 4), "combinations_timed": combos}
+    del graph, slab_graph, progs, slab_progs, runners
+    torch.cuda.empty_cache()
+    return res
+
+
 def cpu_baseline_chain(st, threads):
     """The C oracle (scalar restatement of the reference semantics) on the host cores over the
     same packed inputs: count + sum of the chain; also checks the GPU result."""
@@ -617,6 +719,10 @@ def run_gpu(args):
                 extra["batched_512"] = batched_512(dev, args.steps)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["batched_512"] = {"error": str(e)}
+            try:
+                extra["mixed_chain"] = mixed_chain(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["mixed_chain"] = {"error": str(e)}
             for name, kw in [("chain_50pct", {"thresh": 4160}), ("chain_plain32_in", {"a_fmt": 0, "b_fmt": 0}),
                              ("chain_plain32_out", {"out_fmt": 0}),
                              ("chain_plain32_in_out", {"a_fmt": 0, "b_fmt": 0, "out_fmt": 0})]:
@@ -685,9 +791,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="amethyst", choices=["amethyst", "reference"])
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--only", default=None, help="run one secondary workload by name and print it")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        import torch
+
+        torch.cuda.set_device(0)
+        fn = {"mixed_chain": mixed_chain, "batched_512": batched_512, "groupby_2e28": groupby_2e28,
+              "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1}[args.only]
+        print(json.dumps({args.only: fn(torch.device("cuda", 0), args.steps)}), flush=True)
     else:
         run_gpu(args)
 

@@ -142,6 +142,15 @@ typedef struct {
 amx_status amx_set_tuning(const amx_tuning* t);
 amx_status amx_get_tuning(amx_tuning* t);
 
+/* Test hook for the failure path (no reference counterpart; the reference prints and exits,
+ * src/cuda_try.cuh:8-21).  For the tile-pipeline launches this host thread makes next, the kernel
+ * never publishes the look-back count of tile `tile`, and every look-back poll loop gives up after
+ * `wait_polls` polls (0: the built-in bound of 2^20).  The waits on that tile then run out: the
+ * kernel records AMX_ERR_TIMEOUT, takes the missing count as 0, finishes (its compacted outputs
+ * are invalid), and amx_workspace_status() reports the timeout.  Nothing faults or hangs.
+ * tile = UINT64_MAX switches the hook off. */
+amx_status amx_test_lookback_timeout(uint64_t tile, uint32_t wait_polls);
+
 /* ---- column operators ------------------------------------------------------------------ */
 
 /* filter -> bitmask.  Replaces kernel_filter_{slabs,nogaps,baseline}
@@ -172,6 +181,12 @@ amx_status amx_filter_compressstore(const amx_column* in, const amx_predicate* p
  * stream capture starts.  Calls no cudaMalloc, cudaFree or allocating library routine. */
 amx_status amx_filter_compressstore_noalloc(const amx_column* in, const amx_predicate* pred, const amx_column* out,
                                             uint64_t* d_count, void* stream);
+/* synchronises `stream`, then reports a device-side failure (AMX_ERR_TIMEOUT: the outputs are
+ * invalid) recorded by the last amx_filter_compressstore_noalloc call on the current device;
+ * AMX_OK if none.  The next no-alloc call clears the record, so check before making it.  The
+ * array's address is looked up once per device: do not call either no-alloc entry point on a
+ * device after cudaDeviceReset in the same process. */
+amx_status amx_filter_compressstore_noalloc_status(void* stream);
 
 /* element-wise binary op, lhs and rhs may differ in format and width.  Replaces
  * kernel_binary_op_{slabs,nogaps,baseline} (src/kernels/binary_op_slabs.cuh:7-67,
@@ -278,6 +293,89 @@ typedef struct {
 amx_status amx_chain(const amx_chain_desc* desc, const amx_column* lhs, const amx_column* rhs, const amx_column* out,
                      uint32_t* d_mask, uint64_t* d_count, uint64_t* d_agg, void* workspace, size_t workspace_bytes,
                      void* stream);
+
+/* ---- operator-chain programs ------------------------------------------------------------- */
+/* A program runs a chain of steps over one column x with no host round trip: every length a
+ * step produces (a compressstore's survivor count) stays in device memory and the following
+ * kernels read it there, so a program is a fixed sequence of stream-ordered launches that can
+ * be captured into a CUDA graph.  State: the column x (initially the input), its length len,
+ * and the live filter mask (initially none).  Steps:
+ *   FILTER         mask = pred(x[0..len))
+ *   COMPRESSSTORE  x = the elements of x whose mask bit is set (pred(x) when no mask is live),
+ *                  stored as out_format / out_bits; len = their count; no mask is live after it
+ *   BINARY         x = op(x, aux[0..len)) masked to value_bits, stored as out_format / out_bits;
+ *                  the mask stays live.  out_format AMX_FORMAT_FUSED (only before a
+ *                  COMPRESSSTORE) runs the op inside that step's pass: no intermediate
+ *   REDUCE         *d_result = op (an amx_agg) over x[0..len) (the masked elements if a mask is
+ *                  live)
+ *   GROUPBY        group-by sum + count of x[0..len) by the keys aux[0..len) (masked if a mask
+ *                  is live) into group_keys / group_sums / group_counts (any may have NULL data;
+ *                  capacity >= 2^aux.bits), the number of groups into *d_result; keys <= 24 bits
+ * Steps that one pass can serve run as one: a FILTER directly before a COMPRESSSTORE becomes its
+ * predicate, and a REDUCE directly after a COMPRESSSTORE, a FILTER, or a BINARY op with no live
+ * mask is computed in that step's pass.  AMX_FORMAT_FUSED may also precede FILTER, COMPRESSSTORE.
+ * A storage width narrower than the values keeps their low bits: choose one only for values
+ * known to fit.  aux columns hold at least x.n elements; the first len of them are used.  The
+ * reference runs operators one after another with a host-side count between them
+ * (src/op_chaining_demo.cu:137-152, src/benchs/bench_compressstore_slabs.cu:60-62); programs have
+ * no reference counterpart. */
+typedef enum {
+    AMX_STEP_FILTER = 0,
+    AMX_STEP_COMPRESSSTORE = 1,
+    AMX_STEP_BINARY = 2,
+    AMX_STEP_REDUCE = 3,
+    AMX_STEP_GROUPBY = 4
+} amx_step_kind;
+
+#define AMX_FORMAT_FUSED 0xffu
+#define AMX_PROGRAM_MAX_STEPS 32
+
+typedef struct {
+    uint32_t kind;
+    uint32_t op;          /* BINARY: amx_binop; REDUCE: amx_agg */
+    uint32_t value_bits;  /* BINARY: width the result is masked to */
+    uint32_t out_format;  /* BINARY, COMPRESSSTORE: storage of the new x (AMX_FORMAT_FUSED: none) */
+    uint32_t out_bits;    /* BINARY, COMPRESSSTORE: storage width of the new x */
+    uint32_t reserved;
+    amx_predicate pred;   /* FILTER; COMPRESSSTORE when no mask is live */
+    amx_column aux;       /* BINARY: right operand; GROUPBY: keys */
+    uint64_t* d_result;   /* REDUCE: the aggregate; GROUPBY: the number of groups; COMPRESSSTORE: the
+                           * survivor count (GROUPBY, COMPRESSSTORE: may be NULL) */
+    amx_column group_keys;
+    amx_column group_sums;
+    amx_column group_counts;
+} amx_step;
+
+typedef struct amx_program amx_program;
+
+/* validates the steps and plans the workspace (host only; the step array is copied) */
+amx_status amx_program_create(const amx_column* x, const amx_step* steps, uint32_t nsteps, amx_program** prog);
+/* device workspace a run needs (256-byte aligned, reusable by consecutive runs on one stream) */
+uint64_t amx_program_workspace_bytes(const amx_program* prog);
+/* enqueues every step on `stream`: no synchronisation, no allocation, capturable */
+amx_status amx_program_run(const amx_program* prog, void* workspace, size_t workspace_bytes, void* stream);
+/* the final x of the last run: its column (data inside the workspace or the input's own; n = the
+ * capacity) and a device pointer to its length (NULL when no step changes the length: x->n) */
+amx_status amx_program_output(const amx_program* prog, const void* workspace, amx_column* x, const uint64_t** d_len);
+/* synchronises `stream`, then reports a device-side failure recorded by the last run */
+amx_status amx_program_status(const amx_program* prog, const void* workspace, void* stream);
+void amx_program_destroy(amx_program* prog);
+
+/* Many programs in one CUDA graph: program i runs on lane i's stream (lanes assigned longest
+ * first to the least loaded lane), lanes fork from and join the launching stream, so the
+ * programs of different lanes overlap on the GPU.  Each program needs its own workspace.  The
+ * capture uses internal streams; launching replays every program with no host work per step. */
+typedef struct amx_graph amx_graph;
+amx_status amx_graph_capture(const amx_program* const* progs, void* const* workspaces, const uint64_t* workspace_bytes,
+                             uint32_t count, uint32_t lanes, amx_graph** graph);
+amx_status amx_graph_launch(const amx_graph* graph, void* stream);
+void amx_graph_destroy(amx_graph* graph);
+
+/* ---- column statistics ------------------------------------------------------------------- */
+/* d_hist[k] += number of elements whose value needs exactly k bits (k = 0 for the value 0),
+ * k = 0..64 (65 uint64 counters, caller-cleared) -- the bit-width histogram the format selector
+ * reads.  No reference counterpart. */
+amx_status amx_bit_histogram(const amx_column* in, uint64_t* d_hist, void* stream);
 
 /* ---- learned format selector ------------------------------------------------------------- */
 /* A 16 -> 64 -> 64 -> classes FP32 MLP (ReLU, softmax) that picks storage formats and widths for

@@ -26,6 +26,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "amethyst.h"
 
@@ -173,5 +174,69 @@ void hop(amx_format fmt, uint64_t* d_data, size_t n, uint64_t* d_out, amx_agg ag
     void* ws = workspace(n, &wb);
     check(amx_reduce(agg, &in, nullptr, d_out, ws, wb, s));
 }
+
+// ---- operator-chain programs and graphs (amx_program_*, amx_graph_*) -------------------------
+// RAII owners: a program plans its steps and holds its device workspace (cudaMalloc once, at
+// construction); a graph captures programs once and replays them.  The reference has no
+// counterpart: it runs operators one at a time (src/op_chaining_demo.cu:137-152).
+class program {
+  public:
+    program(const amx_column& x, const std::vector<amx_step>& steps)
+    {
+        check(amx_program_create(&x, steps.data(), (uint32_t)steps.size(), &p_));
+        bytes_ = (size_t)amx_program_workspace_bytes(p_);
+        if (cudaMalloc(&ws_, bytes_) != cudaSuccess) {
+            amx_program_destroy(p_);
+            throw error(AMX_ERR_CUDA, "program workspace allocation failed");
+        }
+    }
+    program(const program&) = delete;
+    program& operator=(const program&) = delete;
+    ~program()
+    {
+        cudaFree(ws_);
+        amx_program_destroy(p_);
+    }
+    void run(cudaStream_t s = 0) { check(amx_program_run(p_, ws_, bytes_, s)); }
+    // the final column of the last run and a device pointer to its length (nullptr: x.n)
+    amx_column output(const uint64_t** d_len) const
+    {
+        amx_column c{};
+        check(amx_program_output(p_, ws_, &c, d_len));
+        return c;
+    }
+    void status(cudaStream_t s = 0) const { check(amx_program_status(p_, ws_, s)); }
+    const amx_program* get() const { return p_; }
+    void* workspace() const { return ws_; }
+    uint64_t workspace_bytes() const { return bytes_; }
+
+  private:
+    amx_program* p_ = nullptr;
+    void* ws_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+class graph {
+  public:
+    graph(const std::vector<const program*>& progs, uint32_t lanes)
+    {
+        std::vector<const amx_program*> h;
+        std::vector<void*> ws;
+        std::vector<uint64_t> wb;
+        for (const program* p : progs) {
+            h.push_back(p->get());
+            ws.push_back(p->workspace());
+            wb.push_back(p->workspace_bytes());
+        }
+        check(amx_graph_capture(h.data(), ws.data(), wb.data(), (uint32_t)h.size(), lanes, &g_));
+    }
+    graph(const graph&) = delete;
+    graph& operator=(const graph&) = delete;
+    ~graph() { amx_graph_destroy(g_); }
+    void launch(cudaStream_t s = 0) const { check(amx_graph_launch(g_, s)); }
+
+  private:
+    amx_graph* g_ = nullptr;
+};
 
 }  // namespace amethyst

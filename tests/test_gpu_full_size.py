@@ -1,17 +1,18 @@
-"""Every benchmark configuration at its full size, checked bit-exactly: against the C oracle where
-it finishes in seconds (the 2^24-element filter + compressstore, the 2^26-element operator
-chain), and elsewhere through properties that hold at any size, with plain torch integer ops on
-the unpacked values as the independent side:
-  - the 1 GiB column (671,088,640 elements of 11 bits): encode -> decode round trip; the
-    compacted column decodes to torch.masked_select of the values; its count equals the
-    popcount of the filter's bitmask and the count of the count-only chain; the chain's sum
-    equals the torch sum of the survivors;
-  - the operator chain over {packed, plain} inputs x {packed, plain} outputs;
-  - the 2^28-element group-by: per-group sums (index_add_) and counts (bincount), counts summing
-    to n;
-  - the 4096^3 u7 matrix product: against an fp64 product (exact below 2^53), and the
-    narrowest width the output needs;
+"""Every benchmark configuration at its full size, checked bit-exactly against the C oracle:
+  - the 2^24-element filter + compressstore (also against the reference's own kernels);
+  - the 1 GiB column (671,088,640 elements of 11 bits), encoded on the host by the oracle: the
+    compacted bytes and the count against the oracle's filter + compressstore, whole buffer;
+    plus properties with plain torch integer ops as an independent side (encode -> decode round
+    trip of the device encoder, masked_select, bitmask popcount, count-only chain, sum);
+  - the 2^26-element operator chain (and, through torch, its {packed, plain} x {packed, plain}
+    forms);
+  - the 2^28-element group-by against the oracle's dense-array group-by (and torch
+    index_add_ / bincount);
+  - the 4096^3 u7 matrix product: a 256-row block against the oracle's exact int64 product, the
+    whole product against an fp64 product (exact below 2^53), and the narrowest output width;
   - 512 uneven columns in one batch: per-column count, sum and decoded output."""
+import os
+
 import numpy as np
 import pytest
 
@@ -93,6 +94,29 @@ def test_cfg1_filter_compressstore_vs_oracle(cuda):
                                                   C.c_void_p(rout.data_ptr()), n, C.byref(rc), 1024) == 0
         assert rc.value == wcnt
         assert np.array_equal(O.decode(rout[:nb].cpu().numpy(), wcnt, SLAB, 11), O.decode(want[:nb], wcnt, SLAB, 11))
+
+
+def test_one_gib_column_vs_oracle(cuda):
+    """The north-star column encoded on the host by the oracle (not by the device encoder),
+    filtered v < 205 and compressstored on the GPU: the whole compacted buffer and the count
+    against the oracle.  At 671,088,640 elements this covers the 64-bit index paths."""
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import datagen, ops
+
+    n = (1 << 27) * 5
+    raw = O.encode(SLAB, 11, datagen.uniform_np(0xC0FFEE, 11, n))
+    nb = O.storage_bytes(SLAB, 11, n)
+    assert nb == 1 << 30
+    col = ops.PackedColumn.empty(n, SLAB, 11)
+    col.data[:nb].copy_(torch.from_numpy(raw[:nb]))
+    out, cnt = ops.filter_compressstore(col, ops.predicate(A.PRED_LT, 205, 0, 11), SLAB, 11)
+    want, wcnt = O.filter_compressstore(raw, n, SLAB, 11, O.pred(A.PRED_LT, 205), SLAB, 11)
+    del raw
+    assert int(cnt[0].item()) == wcnt
+    ob = O.storage_bytes(SLAB, 11, wcnt)
+    assert np.array_equal(out.data[:ob].cpu().numpy(), want[:ob])
 
 
 def test_one_gib_column_properties(cuda):
@@ -185,6 +209,15 @@ def test_groupby_full_size(cuda):
     assert torch.equal(ok.data[: 4 * g].view(torch.int32).long(), present)
     assert torch.equal(osum.data[: 8 * g].view(torch.int64), want_sum[present])
     assert torch.equal(ocnt.data[: 8 * g].view(torch.int64), want_cnt[present])
+    # the oracle's dense-array group-by over the same packed bytes
+    kraw = keys.data[: keys.nbytes].cpu().numpy()
+    vraw = vals.data[: vals.nbytes].cpu().numpy()
+    og, osums, ocounts = O.groupby_dense(kraw, SLAB, 10, vraw, SLAB, 16, n)
+    opresent = np.nonzero(ocounts)[0]
+    assert og == g
+    assert np.array_equal(ok.data[: 4 * g].view(torch.int32).cpu().numpy(), opresent.astype(np.int32))
+    assert np.array_equal(osum.data[: 8 * g].cpu().numpy().view(np.uint64), osums[opresent])
+    assert np.array_equal(ocnt.data[: 8 * g].cpu().numpy().view(np.uint64), ocounts[opresent])
 
 
 def test_matmul_full_size(cuda):
@@ -209,6 +242,11 @@ def test_matmul_full_size(cuda):
     want = torch.matmul(ta, tb).long()
     got = out.data[: 4 * m * n].view(torch.int32).long().reshape(m, n)
     assert torch.equal(got, want)
+    # rows 1024..1279 against the oracle's exact int64 product
+    r0, rows = 1024, 256
+    ablk = O.matrix_encode(SLAB, 7, av[r0 * k:(r0 + rows) * k], rows, k)
+    oc = O.matmul(ablk, SLAB, 7, braw, SLAB, 7, rows, n, k, threads=os.cpu_count() or 1)
+    assert np.array_equal(got[r0:r0 + rows].cpu().numpy(), oc)
     _, w = ops.matmul(a, b, m, n, k, out_fmt=SLAB, out_bits=0)
     assert int(w[0].item()) == int(want.max().item()).bit_length()
 

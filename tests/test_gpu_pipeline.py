@@ -332,3 +332,53 @@ def test_chain_plain_generic_kernel(cuda, lf, lb, rf, rb, op):
                 if want_agg:
                     assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (lf, lb, rf, rb, op, n, agg)
                 assert np.array_equal(gpu_bytes(out, c), wout), (lf, lb, rf, rb, op, n, agg, of)
+
+
+# The runtime-format map variant (12 elements per thread) serves element-wise outputs only where
+# its stage pair and output slot fit in 220 KB: 5632 + slot + 2 * stage <= 225280 bytes, with
+# slot = 6144 * (2 or 8) bytes and stage = the staged bytes of both inputs for 6144 elements.
+# These cases sit on both sides of that line (the other side runs the 8-element kernel), with
+# ragged lengths, so both kernels are pinned to the oracle.
+MAP_FIT_CASES = [
+    # op, lhs (fmt, bits), rhs (fmt, bits) or None, out (fmt, bits), fits
+    (None, (PLAIN64, 64), None, (PLAIN64, 64), True),                   # convert: 153,344 B
+    (0, (PLAIN64, 64), (PLAIN32, 32), (PLAIN64, 64), True),             # 202,752 B
+    (0, (PLAIN64, 64), (NOGAPS, 40), (NOGAPS, 64), True),               # 215,040 B
+    (9, (PLAIN64, 64), (NOGAPS, 48), (PLAIN64, 64), False),             # 227,328 B
+    (0, (PLAIN64, 64), (PLAIN64, 63), (SLAB, 64), False),               # 251,904 B
+    (2, (SLAB, 33), (PLAIN64, 30), (NOGAPS, 63), False),                # 251,904 B
+    (1, (NOGAPS, 60), (PLAIN32, 16), (PLAIN32, 16), True),              # 16-bit slot
+]
+
+
+@pytest.mark.parametrize("case", range(len(MAP_FIT_CASES)))
+@pytest.mark.parametrize("n", [6144 * 3 + 1, 6144 * 5 - 1, 100003])
+def test_map_variant_fit_boundary(cuda, case, n):
+    from amethyst_b200 import ops
+
+    op, (lf, lb), rhs, (of, ob), _ = MAP_FIT_CASES[case]
+    lv, lraw = make_column(case * 101 + n, lf, lb, n)
+    lc = to_gpu(lraw, n, lf, lb)
+    if rhs is None:
+        out = ops.convert(lc, of, ob)
+        want = O.binary(13, lraw, lf, lb, lraw, lf, lb, n, of, ob)  # LHS = identity
+    else:
+        rf, rb = rhs
+        rv, rraw = make_column(case * 103 + n, rf, rb, n)
+        out = ops.binary_op(op, lc, to_gpu(rraw, n, rf, rb), of, ob)
+        want = O.binary(op, lraw, lf, lb, rraw, rf, rb, n, of, ob)
+    assert np.array_equal(gpu_bytes(out), want), (MAP_FIT_CASES[case], n)
+
+
+def test_map_fit_table_matches_the_rule():
+    """The byte counts behind MAP_FIT_CASES, recomputed from the staging rule."""
+    def stage(fmt, bits, t=6144):
+        b = {PLAIN32: 4 * t, PLAIN64: 8 * t, SLAB: 8 * (t // (64 // bits) + 2),
+             NOGAPS: 8 * (t * bits // 64 + 2)}[fmt]
+        return (b + 48 + 127) // 128 * 128
+
+    for op, (lf, lb), rhs, (of, ob), fits in MAP_FIT_CASES:
+        vbits = ob
+        st = stage(lf, lb) + (stage(*rhs) if rhs else 0)
+        slot = (6144 * (2 if vbits <= 16 else 8) + 127) // 128 * 128
+        assert (5632 + slot + 2 * st <= 225280) == fits, (lf, lb, rhs, of, ob)

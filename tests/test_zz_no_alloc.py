@@ -66,3 +66,39 @@ def test_noalloc_rejects_columns_over_the_scratch_limit(cuda):
     p = A.Predicate(A.PRED_LT, 11, 205, 0)
     assert f(C.byref(big), C.byref(p), C.byref(out), C.c_void_p(0x30000), None) == 7
     assert b"2^29" in A.lib().amx_last_error()
+
+
+def test_noalloc_status_reports_a_device_side_timeout(cuda):
+    """A bounded look-back wait made to run out (amx_test_lookback_timeout) on the no-alloc path
+    is reported by amx_filter_compressstore_noalloc_status; the next call clears the record and
+    is bit-exact again."""
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import build, ops
+
+    h = C.CDLL(build.LIB)
+    status = h.amx_filter_compressstore_noalloc_status
+    status.restype = C.c_int
+    status.argtypes = [C.c_void_p]
+    f = _noalloc_entry()
+    L = A.lib()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n = 1 << 21
+    v, raw = make_column(4242, SLAB, 11, n)
+    col = to_gpu(raw, n, SLAB, 11)
+    p = ops.predicate(A.PRED_LT, 205, 0, 11)
+    want_out, want_cnt = ops.filter_compressstore(col, p, SLAB, 11)
+    out = ops.PackedColumn.empty(n, SLAB, 11)
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    try:
+        A.check(L.amx_test_lookback_timeout(0, 2000))
+        assert f(C.byref(col.desc), C.byref(p), C.byref(out.desc), C.c_void_p(cnt.data_ptr()), stream) == 0
+        assert status(stream) == 6
+    finally:
+        L.amx_test_lookback_timeout((1 << 64) - 1, 0)
+    assert f(C.byref(col.desc), C.byref(p), C.byref(out.desc), C.c_void_p(cnt.data_ptr()), stream) == 0
+    assert status(stream) == 0
+    c = int(cnt[0].item())
+    assert c == int(want_cnt[0].item())
+    assert np.array_equal(gpu_bytes(out, c), gpu_bytes(want_out, c))
