@@ -348,6 +348,64 @@ ora_chain_result ora_chain_mt(uint32_t op, const ora_column* l, const ora_column
     return res;
 }
 
+/* ora_chain with the survivors also compacted into `out` (any format, at out->bits), on
+ * `threads` threads: each thread keeps the survivors of its element range, the ranges are
+ * concatenated in order and encoded.  Same results as ora_chain. */
+typedef struct {
+    chain_job c;
+    uint64_t* vals;
+} chainc_job;
+
+static void* chainc_worker(void* arg)
+{
+    chainc_job* j = (chainc_job*)arg;
+    chain_job* c = &j->c;
+    ora_chain_result res = {0, agg_identity(c->agg)};
+    uint64_t m = ora_mask_bits(c->vbits);
+    for (uint64_t i = c->begin; i < c->end; i++) {
+        uint64_t v = c->r ? ora_binop(c->op, ora_get(c->l, i), ora_get(c->r, i), c->vbits) : (ora_get(c->l, i) & m);
+        if (ora_pred_eval(c->p, v)) {
+            j->vals[res.count++] = v;
+            res.agg = agg_apply(c->agg, res.agg, v);
+        }
+    }
+    c->res = res;
+    return NULL;
+}
+
+ora_chain_result ora_chain_compress_mt(uint32_t op, const ora_column* l, const ora_column* r, uint32_t vbits,
+                                       const ora_pred* p, uint32_t agg, const ora_column* out, int threads)
+{
+    if (threads < 1) threads = 1;
+    chainc_job* jobs = (chainc_job*)calloc((size_t)threads, sizeof(chainc_job));
+    pthread_t* th = (pthread_t*)calloc((size_t)threads, sizeof(pthread_t));
+    uint64_t n = l->n;
+    for (int t = 0; t < threads; t++) {
+        uint64_t b = n * (uint64_t)t / threads, e = n * (uint64_t)(t + 1) / threads;
+        jobs[t].c = (chain_job){op, l, r, vbits, p, agg, b, e, {0, 0}};
+        jobs[t].vals = (uint64_t*)malloc((e - b + 1) * sizeof(uint64_t));
+        pthread_create(&th[t], NULL, chainc_worker, &jobs[t]);
+    }
+    ora_chain_result res = {0, agg_identity(agg)};
+    for (int t = 0; t < threads; t++) {
+        pthread_join(th[t], NULL);
+        res.count += jobs[t].c.res.count;
+        res.agg = agg_apply(agg, res.agg, jobs[t].c.res.agg);
+    }
+    uint64_t* all = (uint64_t*)malloc((res.count + 1) * sizeof(uint64_t));
+    uint64_t at = 0;
+    for (int t = 0; t < threads; t++) {
+        memcpy(all + at, jobs[t].vals, jobs[t].c.res.count * sizeof(uint64_t));
+        at += jobs[t].c.res.count;
+        free(jobs[t].vals);
+    }
+    ora_encode(out->format, out->bits, all, res.count, out->data);
+    free(all);
+    free(jobs);
+    free(th);
+    return res;
+}
+
 /* group-by sum/count over a dense key space.  The reference's table
  * (src/kernels/groupby_sm_array.cuh:4-59) truncates sums to the key width and
  * does not emit counts; the dense oracle keeps full uint64 sums and counts. */

@@ -116,6 +116,9 @@ ora_chain_result ora_chain_range(uint32_t op, const ora_column* l, const ora_col
 /* threaded CPU baseline: count + aggregate of the chain with `threads` pthreads */
 ora_chain_result ora_chain_mt(uint32_t op, const ora_column* l, const ora_column* r, uint32_t vbits, const ora_pred* p,
                               uint32_t agg, int threads);
+/* ora_chain that also writes the survivors to out (capacity >= l->n), multi-threaded */
+ora_chain_result ora_chain_compress_mt(uint32_t op, const ora_column* l, const ora_column* r, uint32_t vbits,
+                                       const ora_pred* p, uint32_t agg, const ora_column* out, int threads);
 
 /* group-by: dense per-key sums/counts (keys must be < 2^key_bits, key_bits <= 24).
  * Returns the number of distinct keys. */

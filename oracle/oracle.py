@@ -61,6 +61,7 @@ def ora():
             "ora_reduce": (U64, [U32, col, P]),
             "ora_chain": (OraChainResult, [U32, col, col, U32, pred, U32, col]),
             "ora_chain_mt": (OraChainResult, [U32, col, col, U32, pred, U32, C.c_int]),
+            "ora_chain_compress_mt": (OraChainResult, [U32, col, col, U32, pred, U32, col, C.c_int]),
             "ora_groupby_dense": (U64, [col, col, P, P]),
             "ora_matmul": (None, [col, col, U64, U64, U64, P, C.c_int]),
             "ora_matrix_words": (U64, [U32, U32, U64, U64]),
@@ -170,6 +171,17 @@ def chain_mt(op, lcol, rcol, vbits, p, agg, n, threads):
     res = ora().ora_chain_mt(op, C.byref(lc), C.byref(rc) if rc is not None else None, vbits, C.byref(p), agg,
                              threads)
     return int(res.count), int(res.agg)
+
+
+def chain_compress_mt(op, lcol, rcol, vbits, p, agg, out_fmt, out_bits, n, threads):
+    """chain_mt that also compacts the survivors into out_fmt / out_bits: (out bytes, count, agg)."""
+    lc = column(lcol[0], n, lcol[1], lcol[2])
+    rc = column(rcol[0], n, rcol[1], rcol[2]) if rcol is not None else None
+    out = _buf(out_fmt, out_bits, n)
+    oc = column(out, n, out_fmt, out_bits)
+    res = ora().ora_chain_compress_mt(op, C.byref(lc), C.byref(rc) if rc is not None else None, vbits, C.byref(p),
+                                      agg, C.byref(oc), threads)
+    return out[: storage_bytes(out_fmt, out_bits, res.count)], int(res.count), int(res.agg)
 
 
 def groupby_dense(kraw, kfmt, kbits, vraw, vfmt, vbits, n):

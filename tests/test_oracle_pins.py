@@ -81,3 +81,16 @@ def test_compressstore_is_filter_then_select():
     assert c1 == c2 == int((v < 205).sum())
     assert np.array_equal(out1, out2)
     assert np.array_equal(O.decode(out1, c1, O.SLAB, 11), v[v < 205])
+
+
+def test_chain_compress_mt_matches_chain():
+    """The multi-threaded chain with compacted output (the CPU baseline's routine) agrees with the
+    single-threaded oracle chain on counts, aggregates and output bytes."""
+    for n, threads in ((0, 3), (1, 4), (100003, 7), (65536, 1)):
+        a, b = O.uniform_values(5, 7, n), O.uniform_values(6, 13, n)
+        ar, br = O.encode(2, 7, a), O.encode(2, 13, b)
+        for fmt, bits in ((2, 14), (0, 32), (3, 14)):
+            p = O.pred(4, 4160)
+            w = O.chain(0, (ar, 2, 7), (br, 2, 13), 14, p, 0, fmt, bits, n)
+            g = O.chain_compress_mt(0, (ar, 2, 7), (br, 2, 13), 14, p, 0, fmt, bits, n, threads)
+            assert w[1:] == g[1:] and np.array_equal(w[0], g[0])
