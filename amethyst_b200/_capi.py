@@ -45,7 +45,8 @@ class Tuning(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("words_per_thread", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class BatchPlan(C.Structure):
@@ -89,6 +90,8 @@ _SIGS = {
     "amx_reduce": (C.c_int, [C.c_uint32, _COL, _P, _P, _P, C.c_size_t, _P]),
     "amx_chain": (C.c_int, [C.POINTER(ChainDesc), _COL, _COL, _COL, _P, _P, _P, _P, C.c_size_t, _P]),
     "amx_groupby_workspace_bytes": (C.c_uint64, [C.c_uint32]),
+    "amx_groupby_wide_workspace_bytes": (C.c_uint64, [C.c_uint32, C.c_uint64]),
+    "amx_groupby_status": (C.c_int, [_P, C.c_uint32, _P]),
     "amx_groupby": (C.c_int, [_COL, _COL, _P, _COL, _COL, _COL, _P, _P, C.c_size_t, _P]),
     "amx_matmul_workspace_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32]),
     "amx_matmul_out_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,

@@ -6,7 +6,8 @@ tuner only compares times.  Candidates are timed with CUDA events on the current
 warm-up, and the winner is remembered per (device, workload signature) in memory and, when a
 cache path is given, in a small JSON file.
 
-  tune_batch(cols, preds)        -> amx_batch_tuning for a batch of columns (threads, CTAs per SM)
+  tune_batch(cols, preds)        -> amx_batch_tuning for a batch of columns (threads, CTAs per SM,
+                                    slab words per thread = the tile size)
   tune_pipeline(step, cands)     -> amx_tuning for single-column operators (policy, staging)
 """
 from __future__ import annotations
@@ -69,11 +70,12 @@ def batch_signature(cols) -> str:
     return f"batch/{len(cols)}/{total.bit_length()}/{hist}"
 
 
-BATCH_CANDIDATES = [(256, 0), (256, 3), (256, 2), (512, 0), (512, 2), (512, 1)]
+# (threads per CTA, CTAs per SM (0: as many as fit), slab words per thread: the tile size)
+BATCH_CANDIDATES = [(256, 0, 8), (256, 0, 4), (256, 0, 2), (512, 0, 8), (512, 0, 4), (256, 1, 8)]
 
 
 def tune_batch(cols, preds, candidates=BATCH_CANDIDATES, reps: int = 3, cache_path: str | None = None):
-    """Times each (threads, CTAs per SM) candidate on the batch itself; returns
+    """Times each (threads, CTAs per SM, words per thread) candidate on the batch itself; returns
     (best amx_batch_tuning, {candidate: ms})."""
     from .ops import Batch
 
@@ -81,18 +83,18 @@ def tune_batch(cols, preds, candidates=BATCH_CANDIDATES, reps: int = 3, cache_pa
     key = f"{_device_key()}/{batch_signature(cols)}"
     if key in _cache:
         t = _cache[key]["best"]
-        return A.BatchTuning(t[0], t[1]), _cache[key]["times"]
+        return A.BatchTuning(t[0], t[1], t[2]), _cache[key]["times"]
     times = {}
-    for thr, per_sm in candidates:
-        tun = A.BatchTuning(thr, per_sm)
+    for thr, per_sm, wpt in candidates:
+        tun = A.BatchTuning(thr, per_sm, wpt)
         b = Batch(cols, preds, tun)
-        times[f"{thr}x{per_sm}"] = time_fn(b.run, reps=reps, warmup=1)
+        times[f"{thr}x{per_sm}x{wpt}"] = time_fn(b.run, reps=reps, warmup=1)
         del b
     best = min(times, key=times.get)
-    thr, per_sm = (int(x) for x in best.split("x"))
-    _cache[key] = {"best": [thr, per_sm], "times": times}
+    thr, per_sm, wpt = (int(x) for x in best.split("x"))
+    _cache[key] = {"best": [thr, per_sm, wpt], "times": times}
     _store(cache_path)
-    return A.BatchTuning(thr, per_sm), times
+    return A.BatchTuning(thr, per_sm, wpt), times
 
 
 PIPELINE_CANDIDATES = [

@@ -13,6 +13,8 @@ larger than the 126 MB L2 unless the case says otherwise.
   matmul     4096^3 u7 x u7 slab matrices -> narrowest-width slabs (unpack + GEMM + pack)
   batch64    64 slab columns, lengths log-uniform in [2^16, 2^22], widths 1..32: one batch run
   groupby    2^26 Zipf(1.1) keys over 1000 groups at 10 bits, 2^26 u16 values at 16 bits
+  groupby32  2^26 Zipf(1.1) keys drawn from 100,000 random 32-bit keys (32-bit slabs), 2^26 u16
+             values: the wide-key hash table, the 512 MB key bitmap and the ordered extraction
 """
 from __future__ import annotations
 
@@ -138,6 +140,17 @@ def case(name: str, reps: int = 10) -> dict:
         gws = torch.empty(int(L.amx_groupby_workspace_bytes(10)) + 256, dtype=torch.uint8, device="cuda")
         gws = gws[(-gws.data_ptr()) % 256:]
         ms = _time(lambda: ops.groupby(keys, vals, ws=gws), reps)
+        return {"case": name, "ms": ms, "GB_s": (keys.nbytes + vals.nbytes) / ms / 1e6}
+    if name == "groupby32":
+        n, groups = 1 << 26, 100000
+        idx, _ = datagen.keys_from_cdf_gpu(n, datagen.zipf_cdf(groups, 1.1), 5)
+        pool = torch.from_numpy(np.random.default_rng(6).choice(1 << 32, size=groups, replace=False)).cuda()
+        k32 = pool[idx[:n].long()].to(torch.int64).bitwise_and(0xFFFFFFFF).to(torch.int32)
+        keys = ops.convert(ops.PackedColumn(k32.contiguous().view(torch.uint8), n, A.PLAIN32, 32), A.SLAB, 32)
+        vals = _gen(n, 16, 7)
+        gws = ops.groupby_workspace(32, 1 << 17)
+        ms = _time(lambda: ops.groupby(keys, vals, ws=gws, max_groups=1 << 17), reps)
+        ops.groupby_status(gws, 32)
         return {"case": name, "ms": ms, "GB_s": (keys.nbytes + vals.nbytes) / ms / 1e6}
     raise ValueError(f"unknown case {name}")
 

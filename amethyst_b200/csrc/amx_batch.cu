@@ -3,22 +3,24 @@
 //
 // The reference runs one launch per operator and column (src/main.cu:300-340 drives the benches
 // column by column; src/op_chaining_demo.cu:137-152 chains launches).  Here the columns of a batch
-// are cut into tiles of ~16 KB of packed input (fewer bytes for widths below 8), the tiles of all
-// columns form one work list, and persistent CTAs take work items from an atomic ticket.  Per
-// item:
+// are cut into tiles (threads x words-per-thread slab words), the tiles of all columns form one
+// work list in column-major order, and persistent CTAs take work items from an atomic ticket.
+// Per item:
 //   1. the item's column comes from a host-built item -> column map, its tile from the column's
-//      first item;
-//   2. each thread loads its slab words straight from global memory and evaluates the column's
-//      predicate field-parallel (the runtime-mask form of the single-column policy: whole-word
-//      subtractions against the column's repeated bounds);
-//   3. a block scan gives every thread its survivors' places inside the tile;
-//   4. warp 0 runs a decoupled look-back over the column's earlier items (aggregate / inclusive
-//      prefix flags in one status word per item; bounded spins) for the tile's output offset;
-//   5. survivors are gathered in shared memory and re-encoded as slabs of the column's width at
-//      that offset; the block's survivor sum goes to the column's sum with one 64-bit atomic; the
-//      column's last tile writes its count.
-// Work items are handed out in column-major order, so every item's predecessors are already
-// held by running CTAs and the look-back cannot wait on an item that has not started.
+//      first item; each thread issues the loads of its slab words straight from global memory;
+//   2. while those loads are in flight, the CTA encodes the PREVIOUS item's survivors (its
+//      offset is already known, so no other CTA waits on that work);
+//   3. the column's predicate is evaluated field-parallel (the runtime-mask form of the
+//      single-column policy: whole-word subtractions against the column's repeated bounds);
+//   4. a block scan gives every thread its survivors' places inside the tile, and the tile's
+//      count is published for the look-back at once;
+//   5. warp 0 runs a decoupled look-back over the column's earlier items (aggregate / inclusive
+//      prefix flags in one status word per item; bounded spins) while every warp gathers its
+//      survivors into shared memory; the item is encoded in the next iteration (step 2).
+// A ticket is taken only when its item is about to be worked on: a ticket held ahead of time would
+// delay the publication of that item's count, and every later item of its column waits for it.
+// Work items are handed out in column-major order, so every item's predecessors are already held
+// by running CTAs and the look-back cannot wait on an item that has not started.
 #include <vector>
 
 #include "amx_dispatch.h"
@@ -30,8 +32,9 @@ struct BatchCol {
     const unsigned long long* data;
     unsigned long long* out;
     uint64_t n;
-    uint64_t item0;  // first work item of the column
-    uint64_t items;  // work items of the column
+    uint64_t nwords;  // slab words of the column
+    uint64_t item0;   // first work item of the column
+    uint64_t items;   // work items of the column
     uint64_t sw_h, sw_l1, sw_l2;
     uint32_t bits, eps, spt, te;  // te = elements per tile = threads * spt * eps
     uint32_t sw_mode, cv16;
@@ -51,14 +54,15 @@ constexpr uint64_t kBatchVal = kBatchA - 1;
 constexpr uint32_t kBatchMaxSpt = 8;
 // survivors of one tile: u16 for widths <= 16 (at most 64 per thread), else u32 (at most 24 per thread)
 template <uint32_t THREADS>
-constexpr uint32_t batch_cv_bytes() { return THREADS * 128; }
+__host__ __device__ constexpr uint32_t batch_cv_bytes() { return THREADS * 128; }
 
-// slab words per thread for a width: R = spt * eps <= 64 elements, at most 8 words
-inline uint32_t batch_spt(uint32_t bits)
+// slab words per thread for a width: R = spt * eps <= 64 elements, at most `wpt` (<= 8) words
+inline uint32_t batch_spt(uint32_t bits, uint32_t wpt)
 {
     const uint32_t eps = 64 / bits;
     const uint32_t s = 64 / eps;
-    return s < 1 ? 1 : (s > kBatchMaxSpt ? kBatchMaxSpt : s);
+    const uint32_t cap = wpt < 1 ? 1 : (wpt > kBatchMaxSpt ? kBatchMaxSpt : wpt);
+    return s < 1 ? 1 : (s > cap ? cap : s);
 }
 
 __device__ __forceinline__ uint64_t batch_flags(const BatchCol& c, uint64_t x)
@@ -81,6 +85,37 @@ __device__ __forceinline__ uint64_t batch_flags(const BatchCol& c, uint64_t x)
     return f;
 }
 
+// Encodes the gathered survivors of one finished item at its looked-back offset and accounts its
+// sum and, for a column's last item, its count.
+struct BatchPending {
+    unsigned long long* out;
+    uint64_t g0;
+    uint64_t eps_m64;
+    uint32_t total, bits, eps, cv16, last, ci;
+    unsigned long long sum;
+};
+
+template <uint32_t THREADS>
+__device__ __forceinline__ void batch_encode(const BatchPending& q, const uint8_t* cvbuf, uint32_t tid,
+                                             unsigned long long* counts, unsigned long long* sums)
+{
+    OutDev o{};
+    o.data = q.out;
+    o.mask = (1ull << q.bits) - 1;
+    o.format = AMX_SLAB;
+    o.bits = q.bits;
+    o.eps = q.eps;
+    o.eps_m64 = q.eps_m64;
+    if (q.cv16)
+        encode_tile<uint16_t>(o, reinterpret_cast<const uint16_t*>(cvbuf), q.total, q.g0, q.last, tid, THREADS);
+    else
+        encode_tile<uint32_t>(o, reinterpret_cast<const uint32_t*>(cvbuf), q.total, q.g0, q.last, tid, THREADS);
+    if (tid == 0) {
+        if (q.sum) atomicAdd(&sums[q.ci], q.sum);
+        if (q.last) counts[q.ci] = q.g0 + q.total;
+    }
+}
+
 template <uint32_t THREADS>
 __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __restrict__ cols,
                                                            const uint32_t* __restrict__ colmap, uint64_t total_items,
@@ -94,10 +129,12 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
     __shared__ unsigned long long s_wsum[NW];
     __shared__ uint64_t s_excl;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    BatchPending pend{};
+    bool pending = false;
 
     for (;;) {
         if (tid == 0) s_item = atomicAdd(&hdr->ticket, 1ull);
-        __syncthreads();
+        __syncthreads();  // the ticket; also every read of the previous item's shared values is done
         const uint64_t item = s_item;
         if (item >= total_items) break;
         const uint32_t ci = __ldg(colmap + item);
@@ -110,15 +147,15 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
         const uint32_t B = c.bits;
         const uint64_t FM = (1ull << B) - 1;
 
-        // 2. words and field-parallel flags
+        // 1. this item's slab words, loads in flight ...
         uint64_t x[kBatchMaxSpt], g[kBatchMaxSpt];
-        {
-            const uint64_t nslabs = (c.n + c.eps - 1) / c.eps;
-            const uint64_t s0 = t * (uint64_t)(THREADS * c.spt) + (uint64_t)tid * c.spt;
+        const uint64_t s0 = t * (uint64_t)(THREADS * c.spt) + (uint64_t)tid * c.spt;
 #pragma unroll
-            for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
-                x[i] = (i < c.spt && s0 + i < nslabs) ? __ldg(c.data + s0 + i) : 0;
-            }
+        for (uint32_t i = 0; i < kBatchMaxSpt; i++) x[i] = (i < c.spt && s0 + i < c.nwords) ? __ldg(c.data + s0 + i) : 0;
+        // 2. ... while the previous item is encoded (it frees the survivor buffer for this one)
+        if (pending) batch_encode<THREADS>(pend, cvbuf, tid, counts, sums);
+        // 3. field-parallel flags
+        {
             const uint32_t le0 = tid * R;
 #pragma unroll
             for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
@@ -132,7 +169,7 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
 #pragma unroll
         for (uint32_t i = 0; i < kBatchMaxSpt; i++) cnt += __popcll(g[i]);
 
-        // 3. block scan
+        // 4. block scan
         uint32_t incl = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -140,7 +177,7 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
             if (lane >= (uint32_t)o) incl += y;
         }
         if (lane == 31) s_wtot[warp] = incl;
-        __syncthreads();
+        __syncthreads();  // warp totals; the previous item's encode is done everywhere
         uint32_t before = 0, total = 0;
 #pragma unroll
         for (uint32_t w = 0; w < NW; w++) {
@@ -150,7 +187,7 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
         }
         const uint32_t pos0 = before + incl - cnt;
 
-        // 4. decoupled look-back inside the column
+        // 5. decoupled look-back inside the column (warp 0) ...
         if (warp == 0) {
             uint64_t excl = 0;
             if (t == 0) {
@@ -158,11 +195,11 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
             }
             else {
                 if (lane == 0) st_relaxed_u64(&status[item], kBatchA | total);
-                uint64_t j = item;  // items [c.item0, j) remain to be visited
+                uint64_t jj = item;  // items [c.item0, jj) remain to be visited
                 bool done = false;
                 while (!done) {
-                    const bool in = j > c.item0 + lane;
-                    const uint64_t idx = j - 1 - lane;
+                    const bool in = jj > c.item0 + lane;
+                    const uint64_t idx = jj - 1 - lane;
                     uint64_t st = in ? ld_relaxed_u64(&status[idx]) : kBatchP;
                     uint32_t spins = 0;
                     while (in && (st & (kBatchP | kBatchA)) == 0) {
@@ -181,14 +218,14 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
                     for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
                     excl += v;
                     done = pmask != 0;
-                    j = j > 32 ? j - 32 : 0;
+                    jj = jj > 32 ? jj - 32 : 0;
                 }
                 if (lane == 0) st_relaxed_u64(&status[item], kBatchP | (excl + total));
             }
             if (lane == 0) s_excl = excl;
         }
 
-        // 5. gather, sum
+        // ... while every warp gathers its survivors and sums them
         unsigned long long mysum = 0;
         {
             uint32_t pos = pos0;
@@ -224,27 +261,22 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
         if (lane == 0) s_wsum[warp] = mysum;
         __syncthreads();  // survivors gathered, s_excl and the warp sums visible
 
-        const uint64_t g0 = s_excl;
-        const bool last = t + 1 == c.items;
-        OutDev o{};
-        o.data = c.out;
-        o.mask = FM;
-        o.format = AMX_SLAB;
-        o.bits = B;
-        o.eps = c.eps;
-        o.eps_m64 = c.eps_m64;
-        if (c.cv16)
-            encode_tile<uint16_t>(o, reinterpret_cast<const uint16_t*>(cvbuf), total, g0, last, tid, THREADS);
-        else
-            encode_tile<uint32_t>(o, reinterpret_cast<const uint32_t*>(cvbuf), total, g0, last, tid, THREADS);
-        if (tid == 0) {
-            unsigned long long s = 0;
-            for (uint32_t w = 0; w < NW; w++) s += s_wsum[w];
-            if (s) atomicAdd(&sums[ci], s);
-            if (last) counts[ci] = g0 + total;
-        }
-        __syncthreads();  // the buffer is free for the next item
+        // the encode waits for the next item's loads to be in flight (step 2)
+        pend.out = c.out;
+        pend.g0 = s_excl;
+        pend.eps_m64 = c.eps_m64;
+        pend.total = total;
+        pend.bits = B;
+        pend.eps = c.eps;
+        pend.cv16 = c.cv16;
+        pend.last = t + 1 == c.items;
+        pend.ci = ci;
+        pend.sum = 0;
+        if (tid == 0)
+            for (uint32_t w = 0; w < NW; w++) pend.sum += s_wsum[w];
+        pending = true;
     }
+    if (pending) batch_encode<THREADS>(pend, cvbuf, tid, counts, sums);
 }
 
 }  // namespace amx
@@ -273,12 +305,25 @@ BatchLayout batch_layout(uint32_t ncols, uint64_t items)
 }
 
 uint32_t tuned_threads(const amx_batch_tuning* t) { return (t && t->threads == 512) ? 512 : 256; }
+uint32_t tuned_wpt(const amx_batch_tuning* t)
+{
+    return (t && t->words_per_thread) ? (t->words_per_thread > kBatchMaxSpt ? kBatchMaxSpt : t->words_per_thread)
+                                      : kBatchMaxSpt;
+}
 
-uint64_t column_items(const amx_column& c, uint32_t threads)
+uint64_t column_items(const amx_column& c, uint32_t threads, uint32_t wpt)
 {
     const uint32_t eps = 64 / c.bits;
-    const uint64_t te = (uint64_t)threads * batch_spt(c.bits) * eps;
+    const uint64_t te = (uint64_t)threads * batch_spt(c.bits, wpt) * eps;
     return (c.n + te - 1) / te;
+}
+
+template <uint32_t T>
+cudaError_t batch_attr(uint32_t smem, int* per_sm)
+{
+    cudaError_t e = cudaFuncSetAttribute(batch_fc_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, batch_fc_kernel<T>, T, smem);
+    return e;
 }
 
 }  // namespace
@@ -288,11 +333,11 @@ extern "C" {
 uint64_t amx_batch_workspace_bytes(const amx_column* ins, uint32_t ncols, const amx_batch_tuning* tuning)
 {
     if (!ins) return 0;
-    const uint32_t T = tuned_threads(tuning);
+    const uint32_t T = tuned_threads(tuning), W = tuned_wpt(tuning);
     uint64_t items = 0;
     for (uint32_t i = 0; i < ncols; i++) {
         if (ins[i].format != AMX_SLAB || ins[i].bits < 1 || ins[i].bits > 32) return 0;
-        items += column_items(ins[i], T);
+        items += column_items(ins[i], T, W);
     }
     return batch_layout(ncols, items).total;
 }
@@ -303,7 +348,7 @@ amx_status amx_batch_prepare(const amx_column* ins, const amx_predicate* preds, 
 {
     if (!plan) return fail(AMX_ERR_INVALID_ARG, "batch_prepare: null plan");
     if (ncols && (!ins || !preds || !outs)) return fail(AMX_ERR_INVALID_ARG, "batch_prepare: null column arrays");
-    const uint32_t T = tuned_threads(tuning);
+    const uint32_t T = tuned_threads(tuning), W = tuned_wpt(tuning);
     std::vector<BatchCol> cols(ncols);
     uint64_t items = 0;
     for (uint32_t i = 0; i < ncols; i++) {
@@ -327,7 +372,8 @@ amx_status amx_batch_prepare(const amx_column* ins, const amx_predicate* preds, 
         c.n = a.n;
         c.bits = a.bits;
         c.eps = 64 / a.bits;
-        c.spt = batch_spt(a.bits);
+        c.nwords = (a.n + c.eps - 1) / c.eps;
+        c.spt = batch_spt(a.bits, W);
         c.te = T * c.spt * c.eps;
         c.item0 = items;
         c.items = (a.n + c.te - 1) / c.te;
@@ -358,18 +404,8 @@ amx_status amx_batch_prepare(const amx_column* ins, const amx_predicate* preds, 
 
     int per_sm = 0;
     const int want = (tuning && tuning->ctas_per_sm) ? (int)tuning->ctas_per_sm : 0;
-    if (T == 512) {
-        e = cudaFuncSetAttribute(batch_fc_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)batch_cv_bytes<512>());
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_fc_kernel<512>, 512, batch_cv_bytes<512>());
-    }
-    else {
-        e = cudaFuncSetAttribute(batch_fc_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)batch_cv_bytes<256>());
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_fc_kernel<256>, 256, batch_cv_bytes<256>());
-    }
+    const uint32_t smem = T * 128;
+    e = T == 512 ? batch_attr<512>(smem, &per_sm) : batch_attr<256>(smem, &per_sm);
     if (e != cudaSuccess) return cuda_fail(e, "batch_prepare: occupancy");
     if (per_sm < 1) return fail(AMX_ERR_UNSUPPORTED, "batch: kernel does not fit on an SM");
     if (want > 0 && want < per_sm) per_sm = want;
@@ -405,11 +441,11 @@ amx_status amx_batch_run(const amx_batch_plan* plan, uint64_t* d_counts, uint64_
     auto* cnt = reinterpret_cast<unsigned long long*>(d_counts);
     auto* sum = reinterpret_cast<unsigned long long*>(d_sums);
     if (plan->threads == 512)
-        batch_fc_kernel<512><<<plan->grid, 512, batch_cv_bytes<512>(), s>>>(cols, colmap, plan->items, status, hdr, cnt,
-                                                                          sum);
+        batch_fc_kernel<512><<<plan->grid, 512, batch_cv_bytes<512>(), s>>>(cols, colmap, plan->items, status, hdr,
+                                                                          cnt, sum);
     else
-        batch_fc_kernel<256><<<plan->grid, 256, batch_cv_bytes<256>(), s>>>(cols, colmap, plan->items, status, hdr, cnt,
-                                                                          sum);
+        batch_fc_kernel<256><<<plan->grid, 256, batch_cv_bytes<256>(), s>>>(cols, colmap, plan->items, status, hdr,
+                                                                          cnt, sum);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "batch_run: launch");
     return AMX_OK;

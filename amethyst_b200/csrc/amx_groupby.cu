@@ -22,6 +22,8 @@
 // 2. the groups are extracted: for at most 4096 groups by one CTA (gb_extract_kernel), else with
 //    the tile pipeline itself: mask = filter(count != 0), then compressstore of the key indices,
 //    the sums and the counts into the caller's output columns.
+#include <cstddef>
+
 #include "amx_dispatch.h"
 #include "amx_pipeline.cuh"
 
@@ -49,7 +51,45 @@ struct GbParams {
     unsigned long long* gsum;
     unsigned long long* gcnt;
     const uint64_t* n_dev;  // optional device-resident length (<= n), read by the kernels
+    // keys wider than kGbMaxKeyBits: gsum / gcnt are indexed by the slot of a global open-addressing
+    // hash table (gkey[slot] = key, kGEmpty when free) of gcap_mask + 1 slots instead of by key
+    unsigned long long* gkey;
+    uint64_t gcap_mask;
+    uint32_t gshift;  // 64 - log2(slots)
+    uint32_t* err;    // AMX_ERR_CAPACITY when the table is full
 };
+
+constexpr unsigned long long kGEmpty = ~0ull;
+
+// The global table slot of `key`: its index in the dense table, or -- for wide keys -- the hash
+// slot holding it, claimed with atomicCAS on first sight (linear probing, at most one lap;
+// UINT64_MAX when the table is full).
+__device__ __forceinline__ uint64_t gb_gslot(const GbParams& p, uint32_t key)
+{
+    if (!p.gkey) return key;
+    const uint64_t h = ((uint64_t)key * 0x9E3779B97F4A7C15ull) >> p.gshift;
+    for (uint64_t probe = 0; probe <= p.gcap_mask; probe++) {
+        const uint64_t s = (h + probe) & p.gcap_mask;
+        const uint64_t cur = ld_relaxed_u64(reinterpret_cast<const uint64_t*>(p.gkey + s));
+        if (cur == key) return s;
+        if (cur == kGEmpty) {
+            const unsigned long long prev = atomicCAS(p.gkey + s, kGEmpty, (unsigned long long)key);
+            if (prev == kGEmpty || prev == key) return s;
+        }
+    }
+    return ~0ull;
+}
+
+__device__ __forceinline__ void gb_global_add(const GbParams& p, uint32_t key, uint64_t sum, uint64_t cnt)
+{
+    const uint64_t s = gb_gslot(p, key);
+    if (s == ~0ull) {
+        record_error(p.err, AMX_ERR_CAPACITY);
+        return;
+    }
+    atomicAdd(&p.gsum[s], (unsigned long long)sum);
+    atomicAdd(&p.gcnt[s], (unsigned long long)cnt);
+}
 
 // elements of this run: n, or the device-resident length a previous kernel wrote
 __device__ __forceinline__ uint64_t gb_len(const GbParams& p)
@@ -255,10 +295,10 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
                 if (!((mw >> i) & 1u)) continue;
                 uint32_t slot = key;
                 if (!DENSE) {
-                    slot = gb_probe(tkey, key);
-                    if (slot == kEmptyKey) {  // table crowded: spill to the global table
-                        atomicAdd(&p.gsum[key], (unsigned long long)val);
-                        atomicAdd(&p.gcnt[key], 1ull);
+                    // a crowded table, or the one key that marks free slots: straight to the global table
+                    slot = key == kEmptyKey ? kEmptyKey : gb_probe(tkey, key);
+                    if (slot == kEmptyKey) {
+                        gb_global_add(p, key, val, 1);
                         continue;
                     }
                 }
@@ -282,11 +322,7 @@ __global__ void __launch_bounds__(kGbThreads) groupby_kernel(const __grid_consta
             for (uint32_t i = tid; i < slots; i += blockDim.x) {
                 const uint32_t c = tcnt[i];
                 const uint64_t sum = NOCARRY ? tlo[i] : ((uint64_t)thi[i] << 32) | tlo[i];
-                if (c) {
-                    const uint32_t key = DENSE ? i : tkey[i];
-                    atomicAdd(&p.gsum[key], (unsigned long long)sum);
-                    atomicAdd(&p.gcnt[key], (unsigned long long)c);
-                }
+                if (c) gb_global_add(p, DENSE ? i : tkey[i], sum, c);
                 if (!DENSE) tkey[i] = kEmptyKey;  // each thread clears the slots it flushed
                 tlo[i] = thi[i] = tcnt[i] = 0;
             }
@@ -369,10 +405,10 @@ __global__ void __launch_bounds__(kGbThreads) groupby_phase_kernel(const __grid_
                 const uint32_t val = phase_next(p.v, vr);
                 uint32_t slot = key;
                 if (!DENSE) {
-                    slot = gb_probe(tkey, key);
-                    if (slot == kEmptyKey) {  // table crowded: spill to the global table
-                        atomicAdd(&p.gsum[key], (unsigned long long)val);
-                        atomicAdd(&p.gcnt[key], 1ull);
+                    // a crowded table, or the one key that marks free slots: straight to the global table
+                    slot = key == kEmptyKey ? kEmptyKey : gb_probe(tkey, key);
+                    if (slot == kEmptyKey) {
+                        gb_global_add(p, key, val, 1);
                         continue;
                     }
                 }
@@ -395,11 +431,7 @@ __global__ void __launch_bounds__(kGbThreads) groupby_phase_kernel(const __grid_
             for (uint32_t i = tid; i < slots; i += blockDim.x) {
                 const uint32_t c = tcnt[i];
                 const uint64_t sum = NOCARRY ? tlo[i] : ((uint64_t)thi[i] << 32) | tlo[i];
-                if (c) {
-                    const uint32_t key = DENSE ? i : tkey[i];
-                    atomicAdd(&p.gsum[key], (unsigned long long)sum);
-                    atomicAdd(&p.gcnt[key], (unsigned long long)c);
-                }
+                if (c) gb_global_add(p, DENSE ? i : tkey[i], sum, c);
                 if (!DENSE) tkey[i] = kEmptyKey;
                 tlo[i] = thi[i] = tcnt[i] = 0;
             }
@@ -418,9 +450,7 @@ __global__ void groupby_wide_kernel(const __grid_constant__ GbParams p)
     const uint64_t n = gb_len(p);
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
         if (p.mask && !((__ldg(p.mask + (e >> 5)) >> (e & 31)) & 1u)) continue;
-        const uint32_t key = (uint32_t)load_elem(p.k, e);
-        atomicAdd(&p.gsum[key], (unsigned long long)load_elem(p.v, e));
-        atomicAdd(&p.gcnt[key], 1ull);
+        gb_global_add(p, (uint32_t)load_elem(p.k, e), load_elem(p.v, e), 1);
     }
 }
 
@@ -492,6 +522,124 @@ __global__ void iota_kernel(uint32_t* out, uint64_t n)
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (uint32_t)i;
 }
 
+// ---- extraction for wide keys: hash slots -> ascending keys ----------------------------------
+// The keys of the occupied slots are distinct, so the position of a key in ascending order is the
+// number of present keys below it: mark every present key in a bitmap of the key space, count
+// the bits of every 256-bit group, scan those counts (per 2048-group block, then the block
+// totals), and a key's position is its block's offset + its group's offset inside the block +
+// the set bits before it in its group.
+constexpr uint32_t kGwGroupWords = 8;     // 32-bit bitmap words per group (256 keys)
+constexpr uint32_t kGwBlockGroups = 2048; // groups per scan block
+
+__global__ void gw_mark_kernel(const unsigned long long* gkey, const unsigned long long* gcnt, uint64_t slots,
+                               uint32_t* bitmap)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride)
+        if (gcnt[s]) {
+            const uint32_t key = (uint32_t)gkey[s];
+            atomicOr(bitmap + (key >> 5), 1u << (key & 31));
+        }
+}
+
+// one CTA of 1024 threads per block of 2048 groups: exclusive in-block prefix of the groups'
+// set bits, and the block's total
+__global__ void __launch_bounds__(1024) gw_scan_blocks_kernel(const uint32_t* bitmap, uint64_t groups, uint32_t* gpre,
+                                                              uint64_t* btot)
+{
+    __shared__ uint32_t wt[32];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t g0 = (uint64_t)blockIdx.x * kGwBlockGroups + 2 * tid;
+    uint32_t c[2] = {0, 0};
+    for (int q = 0; q < 2; q++)
+        if (g0 + q < groups) {
+            const uint4* w = reinterpret_cast<const uint4*>(bitmap + (g0 + q) * kGwGroupWords);
+            const uint4 a = w[0], b = w[1];
+            c[q] = __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w) + __popc(b.x) + __popc(b.y) + __popc(b.z) +
+                   __popc(b.w);
+        }
+    const uint32_t mine = c[0] + c[1];
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) wt[warp] = incl;
+    __syncthreads();
+    uint32_t wp = wt[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, wp, o);
+        if (lane >= (uint32_t)o) wp += y;
+    }
+    const uint32_t before = (warp ? __shfl_sync(0xffffffffu, wp, warp - 1) : 0) + incl - mine;
+    if (g0 < groups) gpre[g0] = before;
+    if (g0 + 1 < groups) gpre[g0 + 1] = before + c[0];
+    if (tid == 1023) btot[blockIdx.x] = wp;  // lane 31's inclusive scan of the warp totals: the block's total
+}
+
+// one CTA: exclusive scan of the block totals in place; the grand total is the number of groups
+__global__ void __launch_bounds__(1024) gw_scan_top_kernel(uint64_t* btot, uint64_t blocks, uint64_t* d_groups)
+{
+    __shared__ unsigned long long wt[32];
+    __shared__ unsigned long long carry;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (uint64_t base = 0; base < blocks; base += 1024) {
+        const uint64_t i = base + tid;
+        const unsigned long long v = i < blocks ? btot[i] : 0;
+        unsigned long long incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        if (lane == 31) wt[warp] = incl;
+        __syncthreads();
+        unsigned long long wp = wt[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, wp, o);
+            if (lane >= (uint32_t)o) wp += y;
+        }
+        const unsigned long long before = (warp ? __shfl_sync(0xffffffffu, wp, warp - 1) : 0) + incl - v;
+        const unsigned long long c0 = carry;
+        if (i < blocks) btot[i] = c0 + before;
+        __syncthreads();
+        if (tid == 1023) carry = c0 + wp;  // lane 31's inclusive scan: this round's total
+        __syncthreads();
+    }
+    if (tid == 0) *d_groups = carry;
+}
+
+// every occupied slot writes its key, sum and count at the key's ascending position (plain
+// arrays of `cap` entries; positions at or past cap are counted as a capacity error)
+__global__ void gw_place_kernel(const unsigned long long* gkey, const unsigned long long* gsum,
+                                const unsigned long long* gcnt, uint64_t slots, const uint32_t* bitmap,
+                                const uint32_t* gpre, const uint64_t* boff, uint32_t* okey, uint64_t* osum,
+                                uint64_t* ocnt, uint64_t cap, uint32_t* err)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += stride) {
+        const uint64_t c = gcnt[s];
+        if (!c) continue;
+        const uint32_t key = (uint32_t)gkey[s];
+        const uint64_t w = key >> 5, g = w / kGwGroupWords;
+        uint64_t pos = boff[g / kGwBlockGroups] + gpre[g];
+        for (uint64_t k = g * kGwGroupWords; k < w; k++) pos += __popc(bitmap[k]);
+        pos += __popc(bitmap[w] & ((1u << (key & 31)) - 1u));
+        if (pos >= cap) {
+            record_error(err, AMX_ERR_CAPACITY);
+            continue;
+        }
+        okey[pos] = key;
+        osum[pos] = gsum[s];
+        ocnt[pos] = c;
+    }
+}
+
 // the aggregation kernel for a key / value format pair, table kind and carry handling
 static const void* gb_kernel(bool kslab, bool vslab, bool dense, bool nocarry)
 {
@@ -530,11 +678,82 @@ uint64_t groupby_pipeline_offset(uint32_t key_bits)
     return gb_layout(key_bits).ws;
 }
 
+// Workspace of a wide-key group-by with a `slots`-entry hash table (a power of two):
+//   header (error word, group count) | keys | sums | counts | key bitmap | group prefixes |
+//   block offsets | placed keys | placed sums | placed counts | pipeline workspace
+struct GwLayout {
+    uint64_t hdr, keys, sums, counts, bitmap, gpre, boff, okey, osum, ocnt, ws, total;
+    uint64_t bitmap_words, groups, blocks;
+};
+
+static GwLayout gw_layout(uint32_t kbits, uint64_t slots)
+{
+    GwLayout l{};
+    l.bitmap_words = (1ull << kbits) / 32;
+    l.groups = l.bitmap_words / kGwGroupWords;
+    l.blocks = (l.groups + kGwBlockGroups - 1) / kGwBlockGroups;
+    l.hdr = 0;
+    l.keys = 256;
+    l.sums = align256(l.keys + 8 * slots);
+    l.counts = align256(l.sums + 8 * slots);
+    l.bitmap = align256(l.counts + 8 * slots);
+    l.gpre = align256(l.bitmap + 4 * l.bitmap_words);
+    l.boff = align256(l.gpre + 4 * l.groups);
+    l.okey = align256(l.boff + 8 * l.blocks);
+    l.osum = align256(l.okey + 4 * slots + 16);
+    l.ocnt = align256(l.osum + 8 * slots);
+    l.ws = align256(l.ocnt + 8 * slots);
+    l.total = align256(l.ws + amx_workspace_bytes(slots));
+    return l;
+}
+
+// slots of the largest table that a workspace of `bytes` holds (0 if none of at least 1024)
+static uint64_t gw_slots_for(uint32_t kbits, uint64_t bytes)
+{
+    uint64_t best = 0;
+    for (uint64_t s = 1024; s <= (1ull << 33) && gw_layout(kbits, s).total <= bytes; s <<= 1) best = s;
+    return best;
+}
+
+struct GwHeader {
+    uint32_t err;
+    uint32_t pad;
+    uint64_t groups;
+};
+
 }  // namespace amx
 
 using namespace amx;
 
 extern "C" {
+
+uint64_t amx_groupby_wide_workspace_bytes(uint32_t key_bits, uint64_t max_groups)
+{
+    if (key_bits <= kGbMaxKeyBits || key_bits > 32 || max_groups > (1ull << 32)) return 0;
+    uint64_t slots = 1024;
+    while (slots < 2 * max_groups) slots <<= 1;  // at most half full
+    return gw_layout(key_bits, slots).total;
+}
+
+amx_status amx_groupby_status(const void* workspace, uint32_t key_bits, void* stream)
+{
+    if (!workspace) return fail(AMX_ERR_INVALID_ARG, "groupby_status: null workspace");
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "groupby_status: stream");
+    uint64_t off = ~0ull;
+    if (key_bits > kGbMaxKeyBits)
+        off = 0;  // GwHeader::err
+    else {
+        const uint64_t g = groupby_pipeline_offset(key_bits);
+        if (g != ~0ull) off = g + offsetof(WsHeader, err);
+    }
+    if (off == ~0ull) return AMX_OK;  // groups extracted by one CTA: nothing can fail on the device
+    uint32_t err = 0;
+    e = cudaMemcpy(&err, static_cast<const uint8_t*>(workspace) + off, sizeof(err), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "groupby_status: read");
+    if (err) return fail((amx_status)err, "groupby: device-side failure (%u)", err);
+    return AMX_OK;
+}
 
 uint64_t amx_groupby_workspace_bytes(uint32_t key_bits)
 {
@@ -553,45 +772,12 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
 
 namespace amx {
 
-amx_status groupby_run(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
-                       const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
-                       uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream, const uint64_t* n_dev)
+// Launches the aggregation of keys / values into the global table described by p (dense, or the
+// wide-key hash table when p.gkey is set).
+static amx_status gb_aggregate(GbParams& p, const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                               cudaStream_t s)
 {
-    amx_status st = check_column(keys, "groupby: keys");
-    if (st) return st;
-    if ((st = check_column(vals, "groupby: values"))) return st;
-    if (keys->n != vals->n) return fail(AMX_ERR_INVALID_ARG, "groupby: keys and values lengths differ");
-    if (keys->bits > kGbMaxKeyBits)
-        return fail(AMX_ERR_UNSUPPORTED, "groupby: keys of %u bits (at most %u)", keys->bits, kGbMaxKeyBits);
-    if (((uintptr_t)d_mask) & 15) return fail(AMX_ERR_ALIGNMENT, "groupby: mask not 16-byte aligned");
-    const uint64_t g = 1ull << keys->bits;
-    const amx_column* outs[3] = {out_keys, out_sums, out_counts};
-    const char* names[3] = {"groupby: out_keys", "groupby: out_sums", "groupby: out_counts"};
-    for (int i = 0; i < 3; i++) {
-        if (!outs[i]) continue;
-        if ((st = check_column(outs[i], names[i]))) return st;
-        if (outs[i]->n < g) return fail(AMX_ERR_INVALID_ARG, "%s: capacity below 2^key_bits", names[i]);
-    }
-    const GbLayout L = gb_layout(keys->bits);
-    if (!ws || ws_bytes < L.total)
-        return fail(AMX_ERR_WORKSPACE, "groupby: workspace of %zu bytes, %llu needed", ws_bytes,
-                    (unsigned long long)L.total);
-    if (((uintptr_t)ws) & 255) return fail(AMX_ERR_ALIGNMENT, "groupby: workspace not 256-byte aligned");
-    cudaStream_t s = (cudaStream_t)stream;
-    uint8_t* w = static_cast<uint8_t*>(ws);
-    cudaError_t e = cudaMemsetAsync(w, 0, L.iota, s);  // sums and counts
-    if (e != cudaSuccess) return cuda_fail(e, "groupby: table clear");
-
-    GbParams p{};
-    p.k = col_dev(keys);
-    p.v = col_dev(vals);
-    p.mask = d_mask;
-    p.n = keys->n;
-    p.kbits = keys->bits;
-    p.dense = keys->bits <= kGbDenseBits;
-    p.gsum = reinterpret_cast<unsigned long long*>(w + L.sums);
-    p.gcnt = reinterpret_cast<unsigned long long*>(w + L.counts);
-    p.n_dev = n_dev;
+    cudaError_t e = cudaSuccess;
     if (p.n) {
         if (vals->bits <= 32) {
             const bool nocarry = vals->bits <= kGbNoCarryBits;
@@ -632,6 +818,126 @@ amx_status groupby_run(const amx_column* keys, const amx_column* vals, const uin
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: aggregation launch");
     }
+    return AMX_OK;
+}
+
+// Keys of 25..32 bits: a global hash table sized by the workspace replaces the dense table; the
+// groups come out in ascending key order through the bitmap ranks (gw_*_kernel) and are encoded
+// into the caller's columns by the tile pipeline, reading the group count on the device.
+static amx_status groupby_wide(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                               const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                               uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream, const uint64_t* n_dev)
+{
+    amx_status st = AMX_OK;
+    if (!ws || ((uintptr_t)ws) & 255) return fail(AMX_ERR_ALIGNMENT, "groupby: workspace null or not 256-byte aligned");
+    const uint32_t kbits = keys->bits;
+    const uint64_t slots = gw_slots_for(kbits, ws_bytes);
+    if (!slots)
+        return fail(AMX_ERR_WORKSPACE, "groupby: workspace of %zu bytes holds no hash table (%llu needed at least)",
+                    ws_bytes, (unsigned long long)gw_layout(kbits, 1024).total);
+    const GwLayout L = gw_layout(kbits, slots);
+    const amx_column* outs[3] = {out_keys, out_sums, out_counts};
+    const char* names[3] = {"groupby: out_keys", "groupby: out_sums", "groupby: out_counts"};
+    uint64_t cap = slots;
+    for (int i = 0; i < 3; i++) {
+        if (!outs[i]) continue;
+        if ((st = check_column(outs[i], names[i]))) return st;
+        if (outs[i]->n < cap) cap = outs[i]->n;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    GwHeader* hdr = reinterpret_cast<GwHeader*>(w + L.hdr);
+    cudaError_t e = cudaMemsetAsync(w, 0, 256, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w + L.keys, 0xff, 8 * slots, s);  // every slot free
+    if (e == cudaSuccess) e = cudaMemsetAsync(w + L.sums, 0, L.bitmap + 4 * L.bitmap_words - L.sums, s);
+    if (e != cudaSuccess) return cuda_fail(e, "groupby: table clear");
+
+    GbParams p{};
+    p.k = col_dev(keys);
+    p.v = col_dev(vals);
+    p.mask = d_mask;
+    p.n = keys->n;
+    p.kbits = kbits;
+    p.dense = 0;
+    p.gsum = reinterpret_cast<unsigned long long*>(w + L.sums);
+    p.gcnt = reinterpret_cast<unsigned long long*>(w + L.counts);
+    p.gkey = reinterpret_cast<unsigned long long*>(w + L.keys);
+    p.gcap_mask = slots - 1;
+    p.gshift = 64 - (uint32_t)__builtin_ctzll(slots);
+    p.err = &hdr->err;
+    p.n_dev = n_dev;
+    if ((st = gb_aggregate(p, keys, vals, d_mask, s))) return st;
+
+    uint32_t* bitmap = reinterpret_cast<uint32_t*>(w + L.bitmap);
+    uint32_t* gpre = reinterpret_cast<uint32_t*>(w + L.gpre);
+    uint64_t* boff = reinterpret_cast<uint64_t*>(w + L.boff);
+    uint64_t* groups = d_groups ? d_groups : &hdr->groups;
+    const unsigned grid = (unsigned)(sm_count() * 8);
+    gw_mark_kernel<<<grid, 256, 0, s>>>(p.gkey, p.gcnt, slots, bitmap);
+    gw_scan_blocks_kernel<<<(unsigned)L.blocks, 1024, 0, s>>>(bitmap, L.groups, gpre, boff);
+    gw_scan_top_kernel<<<1, 1024, 0, s>>>(boff, L.blocks, groups);
+    uint32_t* okey = reinterpret_cast<uint32_t*>(w + L.okey);
+    uint64_t* osum = reinterpret_cast<uint64_t*>(w + L.osum);
+    uint64_t* ocnt = reinterpret_cast<uint64_t*>(w + L.ocnt);
+    gw_place_kernel<<<grid, 256, 0, s>>>(p.gkey, p.gsum, p.gcnt, slots, bitmap, gpre, boff, okey, osum, ocnt, cap,
+                                         &hdr->err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "groupby: extraction launch");
+    // the placed groups into the caller's columns (any format), as many as the device count says
+    const amx_column tk{okey, cap, AMX_PLAIN32, 32}, ts{osum, cap, AMX_PLAIN64, 64}, tc{ocnt, cap, AMX_PLAIN64, 64};
+    const amx_column* srcs[3] = {&tk, &ts, &tc};
+    for (int i = 0; i < 3; i++) {
+        if (!outs[i]) continue;
+        ChainReq r{};
+        r.a = srcs[i];
+        r.vbits = outs[i]->bits;
+        r.out = outs[i];
+        r.n_dev = groups;
+        if ((st = run_chain(r, w + L.ws, L.total - L.ws, s))) return st;
+    }
+    return AMX_OK;
+}
+
+amx_status groupby_run(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                       const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                       uint64_t* d_groups, void* ws, size_t ws_bytes, void* stream, const uint64_t* n_dev)
+{
+    amx_status st = check_column(keys, "groupby: keys");
+    if (st) return st;
+    if ((st = check_column(vals, "groupby: values"))) return st;
+    if (keys->n != vals->n) return fail(AMX_ERR_INVALID_ARG, "groupby: keys and values lengths differ");
+    if (keys->bits > 32) return fail(AMX_ERR_UNSUPPORTED, "groupby: keys of %u bits (at most 32)", keys->bits);
+    if (((uintptr_t)d_mask) & 15) return fail(AMX_ERR_ALIGNMENT, "groupby: mask not 16-byte aligned");
+    if (keys->bits > kGbMaxKeyBits)
+        return groupby_wide(keys, vals, d_mask, out_keys, out_sums, out_counts, d_groups, ws, ws_bytes, stream, n_dev);
+    const uint64_t g = 1ull << keys->bits;
+    const amx_column* outs[3] = {out_keys, out_sums, out_counts};
+    const char* names[3] = {"groupby: out_keys", "groupby: out_sums", "groupby: out_counts"};
+    for (int i = 0; i < 3; i++) {
+        if (!outs[i]) continue;
+        if ((st = check_column(outs[i], names[i]))) return st;
+        if (outs[i]->n < g) return fail(AMX_ERR_INVALID_ARG, "%s: capacity below 2^key_bits", names[i]);
+    }
+    const GbLayout L = gb_layout(keys->bits);
+    if (!ws || ws_bytes < L.total)
+        return fail(AMX_ERR_WORKSPACE, "groupby: workspace of %zu bytes, %llu needed", ws_bytes,
+                    (unsigned long long)L.total);
+    if (((uintptr_t)ws) & 255) return fail(AMX_ERR_ALIGNMENT, "groupby: workspace not 256-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t* w = static_cast<uint8_t*>(ws);
+    cudaError_t e = cudaMemsetAsync(w, 0, L.iota, s);  // sums and counts
+    if (e != cudaSuccess) return cuda_fail(e, "groupby: table clear");
+
+    GbParams p{};
+    p.k = col_dev(keys);
+    p.v = col_dev(vals);
+    p.mask = d_mask;
+    p.n = keys->n;
+    p.kbits = keys->bits;
+    p.dense = keys->bits <= kGbDenseBits;
+    p.gsum = reinterpret_cast<unsigned long long*>(w + L.sums);
+    p.gcnt = reinterpret_cast<unsigned long long*>(w + L.counts);
+    p.n_dev = n_dev;
+    if ((st = gb_aggregate(p, keys, vals, d_mask, s))) return st;
     // groups: keys with a nonzero count, ascending
     if (g <= kGbExtractMax) {
         OutDev od[3] = {};

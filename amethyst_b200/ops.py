@@ -154,19 +154,30 @@ def chain(lhs: PackedColumn, rhs: PackedColumn | None, op: int, value_bits: int,
     return out, mask, cnt, ag
 
 
+def groupby_workspace(key_bits: int, max_groups: int | None = None, device="cuda") -> torch.Tensor:
+    """A 256-byte-aligned group-by workspace: the dense table for keys of at most 24 bits, a hash
+    table for `max_groups` distinct keys above that."""
+    if key_bits <= 24:
+        nb = int(lib().amx_groupby_workspace_bytes(key_bits))
+    else:
+        nb = int(lib().amx_groupby_wide_workspace_bytes(key_bits, max_groups or (1 << 20)))
+    return aligned_bytes(nb, 256, device)
+
+
 def groupby(keys: PackedColumn, vals: PackedColumn, key_fmt: int = A.PLAIN32, sum_fmt: int = A.PLAIN64,
             sum_bits: int = 64, count_fmt: int | None = A.PLAIN64, mask: torch.Tensor | None = None, ws=None,
-            stream=None):
+            stream=None, max_groups: int | None = None):
     """Group-by sum + count (kernel_groupby_sm_array's successor): returns (keys, sums, counts,
-    groups tensor) with groups in ascending key order."""
+    groups tensor) with groups in ascending key order.  Keys of 25..32 bits hold up to
+    `max_groups` (default 2^20) distinct keys."""
     dev = keys.data.device
-    g = 1 << keys.bits
+    g = 1 << keys.bits if keys.bits <= 24 else (max_groups or (1 << 20))
     ok = PackedColumn.empty(g, key_fmt, keys.bits if key_fmt != A.PLAIN32 or keys.bits <= 32 else 32, dev)
     os_ = PackedColumn.empty(g, sum_fmt, sum_bits, dev)
     oc = PackedColumn.empty(g, count_fmt, 64 if count_fmt != A.PLAIN32 else 32, dev) if count_fmt is not None else None
     ng = torch.zeros(2, dtype=torch.int64, device=dev)
     if ws is None:
-        ws = torch.empty(int(lib().amx_groupby_workspace_bytes(keys.bits)), dtype=torch.uint8, device=dev)
+        ws = groupby_workspace(keys.bits, max_groups, dev)
     check(lib().amx_groupby(C.byref(keys.desc), C.byref(vals.desc), _ptr(mask), C.byref(ok.desc), C.byref(os_.desc),
                             C.byref(oc.desc) if oc is not None else None, _ptr(ng), _ptr(ws), ws.numel(),
                             _stream_ptr(stream)))
@@ -300,6 +311,10 @@ class Graph:
         if h is not None and h.value:
             lib().amx_graph_destroy(h)
             self.h = None
+
+
+def groupby_status(ws: torch.Tensor, key_bits: int, stream=None) -> None:
+    check(lib().amx_groupby_status(_ptr(ws), key_bits, _stream_ptr(stream)))
 
 
 def workspace_status(ws: torch.Tensor, stream=None) -> None:

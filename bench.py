@@ -349,7 +349,8 @@ def batched_512(dev, steps):
                        "filter + compressstore + sum",
            "elements": int(ns.sum()), "alg_bytes": byts,
            "batched_graph": {"ms": round(ms_b, 4), "GB_s": round(byts / (ms_b * 1e-3) / 1e9, 2),
-                             "tuning": {"threads": tuning.threads, "ctas_per_sm": tuning.ctas_per_sm},
+                             "tuning": {"threads": tuning.threads, "ctas_per_sm": tuning.ctas_per_sm,
+                                        "words_per_thread": tuning.words_per_thread},
                              "autotune_ms": {k: round(v, 4) for k, v in tune_times.items()}},
            "sequential_512_launches": {"ms": round(ms_s, 4), "GB_s": round(byts / (ms_s * 1e-3) / 1e9, 2)},
            "speedup": round(ms_s / ms_b, 3), "results_equal": same}
@@ -485,6 +486,75 @@ def groupby_2e28(dev, steps):
     del keys, vals, gws, res
     torch.cuda.empty_cache()
     return out
+
+
+def cluster_mask(n, sel, clusters, dev):
+    """`clusters` runs of floor(floor(sel * n) / clusters) set bits, run i starting at element
+    i * floor(n / clusters) -- the reference's clustered compressstore masks
+    (src/main.cu:59-101, modes 1 and 2 with 1 and 8 clusters) -- as LSB-first uint32 words."""
+    import torch
+
+    words = (n + 31) // 32
+    m = torch.zeros(words + 4, dtype=torch.int64, device=dev)
+    run = int(sel * n) // clusters
+    for i in range(clusters):
+        a = i * (n // clusters)
+        b = a + run
+        wa, wb = (a + 31) // 32, b // 32
+        if wa < wb:
+            m[wa:wb] = 0xFFFFFFFF
+        for e0, e1 in ((a, min(b, wa * 32)), (max(a, wb * 32), b)):
+            if e0 < e1:
+                w = e0 // 32
+                bits = ((1 << (e1 - w * 32)) - 1) & ~((1 << (e0 - w * 32)) - 1)
+                m[w] |= bits
+    return m.to(torch.int32)
+
+
+def compressstore_masks(dev, steps):
+    """compressstore of 2^27 elements in 11-bit slabs by a given mask, for the reference's mask
+    distributions (src/main.cu:33-108, run.sh:6-22): uniform random bits, one cluster, eight
+    clusters, at selectivities 0.01, 0.1, 0.5 and 0.9; output in 11-bit slabs.  Bytes = packed
+    input + mask + packed output."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = 1 << 27
+    col = pack_gpu(n, 11, 0x3A5C, 2)
+    out = ops.PackedColumn.empty(n, 2, 11)
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    ws = ops.workspace(n)
+    r16 = pack_gpu(n, 16, 0x3A5D, 0)  # independent uniform 16-bit draws for the uniform masks
+    L = A.lib()
+    stream = torch.cuda.current_stream()
+    rows = {}
+    for sel in (0.01, 0.1, 0.5, 0.9):
+        for name, clusters in (("uniform", 0), ("single_cluster", 1), ("multi_cluster_8", 8)):
+            if clusters:
+                mask = cluster_mask(n, sel, clusters, dev)
+            else:
+                mask = ops.filter(r16, ops.predicate(A.PRED_LT, int(round(sel * 65536))), ws=ws)
+
+            def step():
+                A.check(L.amx_compressstore(C.byref(col.desc), C.c_void_p(mask.data_ptr()), C.byref(out.desc),
+                                            C.c_void_p(cnt.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel(),
+                                            C.c_void_p(stream.cuda_stream)))
+
+            reps = max(3, min(steps, 20))
+            tot, _ = time_steps(step, reps, 3, stream)
+            ms = tot / reps
+            c = int(cnt[0].item())
+            byts = storage_bytes(2, 11, n) + 4 * ((n + 31) // 32) + storage_bytes(2, 11, c)
+            rows[f"{name}_{sel}"] = {"ms": round(ms, 4), "GB_s": round(byts / (ms * 1e-3) / 1e9, 1),
+                                     "selectivity": round(c / n, 5)}
+            del mask
+    del col, out, ws, r16
+    torch.cuda.empty_cache()
+    return {"workload": "compressstore by a given mask, 2^27 elements in 11-bit slabs -> 11-bit slabs", "rows": rows}
 
 
 def mixed_chain(dev, steps, chains=64, lanes=8, exhaustive=True):
@@ -722,6 +792,10 @@ def run_gpu(args):
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["batched_512"] = {"error": str(e)}
             try:
+                extra["compressstore_masks"] = compressstore_masks(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["compressstore_masks"] = {"error": str(e)}
+            try:
                 extra["mixed_chain"] = mixed_chain(dev, args.steps)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["mixed_chain"] = {"error": str(e)}
@@ -807,7 +881,8 @@ def main():
         torch.cuda.set_device(0)
         dev = torch.device("cuda", 0)
         fn = {"mixed_chain": lambda d, k: mixed_chain(d, k, lanes=args.lanes), "batched_512": batched_512,
-              "groupby_2e28": groupby_2e28, "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1}[args.only]
+              "groupby_2e28": groupby_2e28, "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1,
+              "compressstore_masks": compressstore_masks}[args.only]
         print(json.dumps({args.only: fn(dev, args.steps)}), flush=True)
     else:
         run_gpu(args)

@@ -207,13 +207,22 @@ amx_status amx_reduce(uint32_t agg, const amx_column* in, const uint32_t* d_mask
 /* ---- group-by ---------------------------------------------------------------------------- */
 /* Group-by sum + count: for every distinct key (ascending) the key, the uint64 sum of its values
  * and its count, compressed into the three output columns (each may be NULL; capacity >=
- * 2^key_bits); the number of groups goes to *d_groups.  Keys: any format, at most 24 bits.
+ * 2^key_bits for keys of at most 24 bits); the number of groups goes to *d_groups.  Keys: any
+ * format, at most 32 bits.  Keys of 25..32 bits aggregate into a global hash table whose size the
+ * workspace sets (amx_groupby_wide_workspace_bytes(key_bits, max_groups) holds max_groups
+ * distinct keys at half load); the groups come out in ascending key order as well, at most as
+ * many as the smallest output capacity, and more distinct keys than the table or the outputs
+ * hold is reported by amx_groupby_status as AMX_ERR_CAPACITY.
  * Values: any format and width.  Optional d_mask restricts the input to the masked elements.
  * Writing sums into a narrower column masks them, which gives the reference's aggregate
  * (sum masked to the key width).  Replaces kernel_groupby_sm_array_gather/_writeout
  * (src/kernels/groupby_sm_array.cuh:4-81) and the sort-based path
  * (src/benchs/bench_groupby_sort_cub.cu:50-63).  The workspace must be 256-byte aligned. */
-uint64_t amx_groupby_workspace_bytes(uint32_t key_bits);
+uint64_t amx_groupby_workspace_bytes(uint32_t key_bits);  /* keys <= 24 bits; 0 otherwise */
+uint64_t amx_groupby_wide_workspace_bytes(uint32_t key_bits, uint64_t max_groups);  /* keys of 25..32 bits */
+/* synchronises `stream`, then reports a device-side failure recorded in `workspace` by the last
+ * amx_groupby with keys of key_bits (AMX_ERR_CAPACITY: a full table or output; AMX_ERR_TIMEOUT) */
+amx_status amx_groupby_status(const void* workspace, uint32_t key_bits, void* stream);
 amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
                        const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
                        uint64_t* d_groups, void* workspace, size_t workspace_bytes, void* stream);
@@ -229,11 +238,13 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
  *   amx_batch_run       clears the outputs and launches the batch: stream-ordered, allocation-free
  *                       and capturable into a CUDA graph, replayable as long as the columns and
  *                       the workspace stay in place.
- * Tuning (may be NULL): threads per CTA (256 or 512) and CTAs per SM (0 = as many as fit). */
+ * Tuning (may be NULL): threads per CTA, CTAs per SM and slab words per thread (the tile size);
+ * the autotuner (amethyst_b200/autotune.py) picks them per workload. */
 typedef struct {
-    uint32_t threads;
-    uint32_t ctas_per_sm;
-    uint32_t reserved[2];
+    uint32_t threads;           /* threads per CTA: 256 or 512 */
+    uint32_t ctas_per_sm;       /* 0: as many as fit */
+    uint32_t words_per_thread;  /* slab words each thread takes per tile, 1..8 (0: 8); sets the tile size */
+    uint32_t reserved;
 } amx_batch_tuning;
 
 typedef struct {

@@ -406,6 +406,48 @@ ora_chain_result ora_chain_compress_mt(uint32_t op, const ora_column* l, const o
     return res;
 }
 
+/* sort-based group-by for keys of any width up to 32 bits: the (key, value) pairs of the masked
+ * elements sorted by key, then reduced by key into ascending keys, uint64 sums and counts -- the
+ * reference's radix-sort + reduce-by-key path (src/benchs/bench_groupby_sort_cub.cu:50-63), with
+ * full uint64 sums and counts emitted.  Returns the number of groups. */
+typedef struct {
+    uint64_t key, val;
+} kv_pair;
+
+static int kv_cmp(const void* a, const void* b)
+{
+    const kv_pair* x = (const kv_pair*)a;
+    const kv_pair* y = (const kv_pair*)b;
+    return x->key < y->key ? -1 : (x->key > y->key ? 1 : 0);
+}
+
+uint64_t ora_groupby_sorted(const ora_column* keys, const ora_column* vals, const uint32_t* mask, uint64_t* out_keys,
+                            uint64_t* out_sums, uint64_t* out_counts)
+{
+    kv_pair* kv = (kv_pair*)malloc((keys->n + 1) * sizeof(kv_pair));
+    uint64_t m = 0;
+    for (uint64_t i = 0; i < keys->n; i++) {
+        if (mask && !((mask[i / 32] >> (i % 32)) & 1u)) continue;
+        kv[m].key = ora_get(keys, i);
+        kv[m].val = ora_get(vals, i);
+        m++;
+    }
+    qsort(kv, m, sizeof(kv_pair), kv_cmp);
+    uint64_t g = 0;
+    for (uint64_t i = 0; i < m; i++) {
+        if (i == 0 || kv[i].key != kv[i - 1].key) {
+            out_keys[g] = kv[i].key;
+            out_sums[g] = 0;
+            out_counts[g] = 0;
+            g++;
+        }
+        out_sums[g - 1] += kv[i].val;
+        out_counts[g - 1]++;
+    }
+    free(kv);
+    return g;
+}
+
 /* group-by sum/count over a dense key space.  The reference's table
  * (src/kernels/groupby_sm_array.cuh:4-59) truncates sums to the key width and
  * does not emit counts; the dense oracle keeps full uint64 sums and counts. */

@@ -122,6 +122,9 @@ ora_chain_result ora_chain_compress_mt(uint32_t op, const ora_column* l, const o
 
 /* group-by: dense per-key sums/counts (keys must be < 2^key_bits, key_bits <= 24).
  * Returns the number of distinct keys. */
+/* sort-based group-by, keys up to 32 bits (the reference's sort + reduce-by-key path) */
+uint64_t ora_groupby_sorted(const ora_column* keys, const ora_column* vals, const uint32_t* mask, uint64_t* out_keys,
+                            uint64_t* out_sums, uint64_t* out_counts);
 uint64_t ora_groupby_dense(const ora_column* keys, const ora_column* vals, uint64_t* sums, uint64_t* counts);
 
 /* matrix multiply: A (M x K), B (K x N) row-major, out int64 (M x N).

@@ -63,6 +63,7 @@ def ora():
             "ora_chain_mt": (OraChainResult, [U32, col, col, U32, pred, U32, C.c_int]),
             "ora_chain_compress_mt": (OraChainResult, [U32, col, col, U32, pred, U32, col, C.c_int]),
             "ora_groupby_dense": (U64, [col, col, P, P]),
+            "ora_groupby_sorted": (U64, [col, col, P, P, P, P]),
             "ora_matmul": (None, [col, col, U64, U64, U64, P, C.c_int]),
             "ora_matrix_words": (U64, [U32, U32, U64, U64]),
             "ora_matrix_encode": (None, [U32, U32, P, U64, U64, P]),
@@ -191,6 +192,17 @@ def groupby_dense(kraw, kfmt, kbits, vraw, vfmt, vbits, n):
     g = ora().ora_groupby_dense(C.byref(column(kraw, n, kfmt, kbits)), C.byref(column(vraw, n, vfmt, vbits)),
                                 _p(sums), _p(counts))
     return int(g), sums, counts
+
+
+def groupby_sorted(kraw, kfmt, kbits, vraw, vfmt, vbits, n, mask=None):
+    """(groups, ascending keys, uint64 sums, uint64 counts) of the masked elements, any key width."""
+    ok = np.zeros(max(n, 1), dtype=np.uint64)
+    os_ = np.zeros(max(n, 1), dtype=np.uint64)
+    oc = np.zeros(max(n, 1), dtype=np.uint64)
+    m = np.ascontiguousarray(mask, dtype=np.uint32) if mask is not None else None
+    g = ora().ora_groupby_sorted(C.byref(column(kraw, n, kfmt, kbits)), C.byref(column(vraw, n, vfmt, vbits)), _p(m),
+                                 _p(ok), _p(os_), _p(oc))
+    return int(g), ok[:g], os_[:g], oc[:g]
 
 
 def matrix_encode(fmt, bits, values: np.ndarray, rows, cols) -> np.ndarray:

@@ -77,7 +77,14 @@ def test_groupby_sizing_and_errors(lib):
     g = C.c_void_p(0x500000)
     call = lambda k, v, w, wb: lib.amx_groupby(C.byref(k), C.byref(v), None, C.byref(out), C.byref(out),  # noqa: E731
                                                C.byref(out), g, w, wb, None)
-    assert call(col(0x100000, 100, A.SLAB, 25), vals, C.c_void_p(0x400000), 1 << 30) == 2  # keys over 24 bits
+    assert call(col(0x100000, 100, A.SLAB, 33), vals, C.c_void_p(0x400000), 1 << 30) == 2  # keys over 32 bits
+    wide = col(0x100000, 100, A.SLAB, 25)
+    assert call(wide, vals, C.c_void_p(0x400000), 4096) == 4                             # no hash table fits
+    assert call(wide, vals, C.c_void_p(0x400010), 1 << 30) == 3                          # not 256-byte aligned
+    w25 = lib.amx_groupby_wide_workspace_bytes(25, 1000)
+    assert w25 > 8 * 2048 * 3 + (1 << 25) // 8 and w25 % 256 == 0                        # 2048 slots, 4 MB bitmap
+    assert lib.amx_groupby_wide_workspace_bytes(24, 1000) == 0                           # dense keys: the other call
+    assert lib.amx_groupby_wide_workspace_bytes(33, 1000) == 0
     assert call(keys, col(0x200000, 99, A.SLAB, 16), C.c_void_p(0x400000), w10) == 1    # lengths differ
     assert call(keys, vals, C.c_void_p(0x400000), w10 - 1) == 4                          # workspace too small
     assert call(keys, vals, C.c_void_p(0x400010), w10) == 3                              # not 256-byte aligned

@@ -43,13 +43,14 @@ def check(batch, want):
         assert np.array_equal(gpu_bytes(batch.outs[i], wcnt), wout), (i, batch.cols[i].n, batch.cols[i].bits)
 
 
-@pytest.mark.parametrize("threads", [256, 512])
-def test_batch_matches_oracle(cuda, threads):
+@pytest.mark.parametrize("threads,wpt", [(256, 8), (512, 8), (256, 3), (512, 1), (256, 2), (512, 5)])
+def test_batch_matches_oracle(cuda, threads, wpt):
+    """Every block shape and tile size (slab words per thread) the autotuner may pick."""
     from amethyst_b200 import _capi as A
     from amethyst_b200 import ops
 
-    cols, preds, want = build(threads, 70)
-    b = ops.Batch(cols, preds, A.BatchTuning(threads, 0))
+    cols, preds, want = build(threads + wpt, 70)
+    b = ops.Batch(cols, preds, A.BatchTuning(threads, 0, wpt))
     b.run()
     check(b, want)
     b.run()  # a second run on the same plan and workspace

@@ -124,3 +124,77 @@ def test_groupby_one_cta_flushes(cuda, kf, kb, vf, vb):
     assert np.array_equal(gpu_bytes(ok, g).view(np.uint32), present.astype(np.uint32))
     assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), want_sum[present])
     assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), want_cnt[present])
+
+
+WIDE_CASES = [
+    # key fmt, key bits, val fmt, val bits, n, distinct keys (0: uniform over the key space)
+    (SLAB, 32, SLAB, 16, 1 << 20, 1000),       # Zipf-weighted draws from 1000 random 32-bit keys
+    (PLAIN32, 32, PLAIN32, 20, 300001, 0),     # nearly every key distinct: ~300K groups
+    (SLAB, 25, NOGAPS, 13, 400003, 0),         # ~4K collisions in a 25-bit space
+    (NOGAPS, 28, SLAB, 7, 123457, 50000),
+    (PLAIN64, 32, PLAIN64, 40, 77777, 3000),   # values wider than 32 bits
+    (SLAB, 30, SLAB, 30, 1, 0),
+    (SLAB, 30, SLAB, 30, 0, 0),
+]
+
+
+def wide_keys(n, bits, distinct, seed):
+    rng = np.random.default_rng(seed)
+    if distinct == 0:
+        k = rng.integers(0, 1 << bits, size=n, dtype=np.uint64)
+    else:
+        pool = rng.choice(1 << bits, size=distinct, replace=False).astype(np.uint64)
+        pool[0] = (1 << bits) - 1  # the all-ones key too
+        k = pool[zipf_keys(n, distinct, 1.1, seed + 1).astype(np.int64)]
+    return k
+
+
+@pytest.mark.parametrize("kf,kb,vf,vb,n,distinct", WIDE_CASES)
+def test_groupby_wide_keys_match_the_sorting_oracle(cuda, kf, kb, vf, vb, n, distinct):
+    """Keys of 25..32 bits: global hash table, groups in ascending key order, against the oracle's
+    sort + reduce-by-key group-by (the reference's sort-based path)."""
+    from amethyst_b200 import ops
+
+    keys = wide_keys(n, kb, distinct, kb + n)
+    kv, kraw = make_column(kb * 11 + n, kf, kb, n, vals=keys)
+    vv, vraw = make_column(vb * 13 + n, vf, vb, n)
+    kc, vc = to_gpu(kraw, n, kf, kb), to_gpu(vraw, n, vf, vb)
+    g, wk, ws, wc = O.groupby_sorted(kraw, kf, kb, vraw, vf, vb, n)
+    cap = max(1024, 2 * g)
+    for key_fmt in (PLAIN32, SLAB):
+        ok, osum, ocnt, ng = ops.groupby(kc, vc, key_fmt=key_fmt, max_groups=cap)
+        gg = int(ng[0].item())
+        assert gg == g
+        assert np.array_equal(gpu_bytes(ok, g), O.encode(key_fmt, kb if key_fmt == SLAB else 32, wk)[
+            : O.storage_bytes(key_fmt, kb if key_fmt == SLAB else 32, g)])
+        assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), ws)
+        assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), wc)
+
+
+def test_groupby_wide_keys_with_mask_and_capacity(cuda):
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n, kb = 200003, 32
+    keys = wide_keys(n, kb, 5000, 9)
+    kv, kraw = make_column(91, SLAB, kb, n, vals=keys)
+    vv, vraw = make_column(92, SLAB, 16, n)
+    kc, vc = to_gpu(kraw, n, SLAB, kb), to_gpu(vraw, n, SLAB, 16)
+    m = np.random.default_rng(5).integers(0, 2**32, size=(n + 31) // 32, dtype=np.uint64).astype(np.uint32)
+    mask = torch.from_numpy(np.concatenate([m, np.zeros(4, np.uint32)]).view(np.int32)).cuda()
+    g, wk, ws, wc = O.groupby_sorted(kraw, SLAB, kb, vraw, SLAB, 16, n, mask=m)
+    wsp = ops.groupby_workspace(kb, 8192)
+    ok, osum, ocnt, ng = ops.groupby(kc, vc, mask=mask, max_groups=8192, ws=wsp)
+    ops.groupby_status(wsp, kb)
+    assert int(ng[0].item()) == g
+    assert np.array_equal(gpu_bytes(ok, g).view(np.uint32), wk.astype(np.uint32))
+    assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), ws)
+    assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), wc)
+    # more distinct keys than the outputs hold: reported, never written past them
+    small = ops.groupby_workspace(kb, 1024)
+    ok2, osum2, ocnt2, ng2 = ops.groupby(kc, vc, max_groups=1024, ws=small)
+    with pytest.raises(A.AmxError) as e:
+        ops.groupby_status(small, kb)
+    assert e.value.status == 7

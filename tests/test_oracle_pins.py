@@ -94,3 +94,24 @@ def test_chain_compress_mt_matches_chain():
             w = O.chain(0, (ar, 2, 7), (br, 2, 13), 14, p, 0, fmt, bits, n)
             g = O.chain_compress_mt(0, (ar, 2, 7), (br, 2, 13), 14, p, 0, fmt, bits, n, threads)
             assert w[1:] == g[1:] and np.array_equal(w[0], g[0])
+
+
+def test_sorted_groupby_matches_dense_groupby():
+    """The oracle's sort + reduce-by-key group-by (wide keys) agrees with its dense-table group-by
+    wherever the dense table fits, with and without a mask."""
+    for n, kb, vb in ((0, 5, 5), (1, 3, 9), (20011, 10, 16), (50000, 16, 33)):
+        k = O.uniform_values(kb + n, kb, n)
+        v = O.uniform_values(vb + n + 1, vb, n)
+        kr, vr = O.encode(2, kb, k), O.encode(3, vb, v)
+        g1, s1, c1 = O.groupby_dense(kr, 2, kb, vr, 3, vb, n)
+        g2, k2, s2, c2 = O.groupby_sorted(kr, 2, kb, vr, 3, vb, n)
+        pres = np.nonzero(c1)[0]
+        assert g1 == g2 and np.array_equal(k2, pres) and np.array_equal(s2, s1[pres]) and np.array_equal(c2, c1[pres])
+        if n:
+            m = np.random.default_rng(n).integers(0, 2**32, size=(n + 31) // 32, dtype=np.uint64).astype(np.uint32)
+            g3, k3, s3, c3 = O.groupby_sorted(kr, 2, kb, vr, 3, vb, n, mask=m)
+            bits = np.unpackbits(m.view(np.uint8), bitorder="little")[:n].astype(bool)
+            kk, vv = k[bits], v[bits]
+            uk = np.unique(kk)
+            assert g3 == len(uk) and np.array_equal(k3, uk)
+            assert np.array_equal(c3, np.array([np.sum(kk == u) for u in uk[:50]] + list(c3[50:]), dtype=np.uint64))
