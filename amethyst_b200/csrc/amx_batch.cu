@@ -21,6 +21,7 @@
 // delay the publication of that item's count, and every later item of its column waits for it.
 // Work items are handed out in column-major order, so every item's predecessors are already held
 // by running CTAs and the look-back cannot wait on an item that has not started.
+#include <type_traits>
 #include <vector>
 
 #include "amx_dispatch.h"
@@ -85,6 +86,45 @@ __device__ __forceinline__ uint64_t batch_flags(const BatchCol& c, uint64_t x)
     return f;
 }
 
+// The survivors of a thread's words in element order into the survivor buffer, and their sum, at
+// the compile-time width B: fully unrolled field tests for dense warps of widths with at most 12
+// fields per slab, a walk over the set flag bits otherwise.
+template <int B>
+__device__ __forceinline__ void batch_gather_ct(const uint64_t (&x)[kBatchMaxSpt], const uint64_t (&g)[kBatchMaxSpt],
+                                                uint32_t spt, bool dense, uint8_t* cvbuf, uint32_t pos,
+                                                unsigned long long& sum)
+{
+    constexpr int EPS = 64 / B;
+    constexpr uint64_t FM = (1ull << B) - 1;
+    using D = typename std::conditional<(B <= 16), uint16_t, uint32_t>::type;
+    D* dst = reinterpret_cast<D*>(cvbuf);
+#pragma unroll
+    for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
+        if (i >= spt) break;
+        if (EPS <= 12 && dense) {
+#pragma unroll
+            for (int k = 0; k < (EPS <= 12 ? EPS : 1); k++)
+                if ((g[i] >> (k * B + B - 1)) & 1) {
+                    const uint32_t v = (uint32_t)((x[i] >> (k * B)) & FM);
+                    dst[pos++] = (D)v;
+                    sum += v;
+                }
+        }
+        else {
+            for (uint64_t f = g[i]; f; f &= f - 1) {
+                const int bp = __ffsll((long long)f) - 1;
+                const uint32_t v = (uint32_t)((x[i] >> (bp - (B - 1))) & FM);
+                dst[pos++] = (D)v;
+                sum += v;
+            }
+        }
+    }
+}
+
+#define AMX_BATCH_WIDTHS(X) \
+    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) \
+    X(20) X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32)
+
 // Encodes the gathered survivors of one finished item at its looked-back offset and accounts its
 // sum and, for a column's last item, its count.
 struct BatchPending {
@@ -106,10 +146,17 @@ __device__ __forceinline__ void batch_encode(const BatchPending& q, const uint8_
     o.bits = q.bits;
     o.eps = q.eps;
     o.eps_m64 = q.eps_m64;
-    if (q.cv16)
-        encode_tile<uint16_t>(o, reinterpret_cast<const uint16_t*>(cvbuf), q.total, q.g0, q.last, tid, THREADS);
-    else
-        encode_tile<uint32_t>(o, reinterpret_cast<const uint32_t*>(cvbuf), q.total, q.g0, q.last, tid, THREADS);
+    switch (q.bits) {  // block-uniform: the compile-time-width encoder of the column's width
+#define AMX_BATCH_ENC(b)                                                                                            \
+    case b:                                                                                                          \
+        encode_slab_ct<b, typename std::conditional<(b <= 16), uint16_t, uint32_t>::type>(                           \
+            o, reinterpret_cast<const typename std::conditional<(b <= 16), uint16_t, uint32_t>::type*>(cvbuf), q.total, \
+            q.g0, q.last, tid, THREADS);                                                                             \
+        break;
+        AMX_BATCH_WIDTHS(AMX_BATCH_ENC)
+#undef AMX_BATCH_ENC
+        default: break;
+    }
     if (tid == 0) {
         if (q.sum) atomicAdd(&sums[q.ci], q.sum);
         if (q.last) counts[q.ci] = q.g0 + q.total;
@@ -117,7 +164,7 @@ __device__ __forceinline__ void batch_encode(const BatchPending& q, const uint8_
 }
 
 template <uint32_t THREADS>
-__global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __restrict__ cols,
+__global__ void __launch_bounds__(THREADS, THREADS == 512 ? 2 : 4) batch_fc_kernel(const BatchCol* __restrict__ cols,
                                                            const uint32_t* __restrict__ colmap, uint64_t total_items,
                                                            uint64_t* status, BatchHdr* hdr,
                                                            unsigned long long* counts, unsigned long long* sums)
@@ -228,32 +275,13 @@ __global__ void __launch_bounds__(THREADS) batch_fc_kernel(const BatchCol* __res
         // ... while every warp gathers its survivors and sums them
         unsigned long long mysum = 0;
         {
-            uint32_t pos = pos0;
             const bool dense = 25 * __reduce_add_sync(0xffffffffu, cnt) > 32 * R;  // above ~4% survivors
-#pragma unroll
-            for (uint32_t i = 0; i < kBatchMaxSpt; i++) {
-                if (dense) {
-                    for (uint32_t k = 0; k < c.eps; k++)
-                        if ((g[i] >> (k * B + B - 1)) & 1) {
-                            const uint32_t v = (uint32_t)((x[i] >> (k * B)) & FM);
-                            if (c.cv16)
-                                reinterpret_cast<uint16_t*>(cvbuf)[pos++] = (uint16_t)v;
-                            else
-                                reinterpret_cast<uint32_t*>(cvbuf)[pos++] = v;
-                            mysum += v;
-                        }
-                }
-                else {
-                    for (uint64_t f = g[i]; f; f &= f - 1) {
-                        const int bp = __ffsll((long long)f) - 1;
-                        const uint32_t v = (uint32_t)((x[i] >> (bp - (B - 1))) & FM);
-                        if (c.cv16)
-                            reinterpret_cast<uint16_t*>(cvbuf)[pos++] = (uint16_t)v;
-                        else
-                            reinterpret_cast<uint32_t*>(cvbuf)[pos++] = v;
-                        mysum += v;
-                    }
-                }
+            switch (B) {  // block-uniform
+#define AMX_BATCH_GATHER(b) \
+    case b: batch_gather_ct<b>(x, g, c.spt, dense, cvbuf, pos0, mysum); break;
+                AMX_BATCH_WIDTHS(AMX_BATCH_GATHER)
+#undef AMX_BATCH_GATHER
+                default: break;
             }
         }
 #pragma unroll

@@ -780,8 +780,11 @@ static amx_status gb_aggregate(GbParams& p, const amx_column* keys, const amx_co
     cudaError_t e = cudaSuccess;
     if (p.n) {
         if (vals->bits <= 32) {
+            // (wide keys with carry words and one flush per CTA measured 4.53 ms against 2.64 ms on
+            // 2^26 keys over 100,000 groups: the returning shared atomics of the carry path cost
+            // more than the flushes into the hash table)
             const bool nocarry = vals->bits <= kGbNoCarryBits;
-            p.flush_every = gb_flush_every(vals->bits);
+            p.flush_every = nocarry ? gb_flush_every(vals->bits) : kGbFlushEvery;
             const uint32_t slots = p.dense ? (1u << p.kbits) : kGbHashSlots;
             const size_t smem = 16ull * slots;
             const void* fn = gb_kernel(keys->format == AMX_SLAB, vals->format == AMX_SLAB, p.dense, nocarry);

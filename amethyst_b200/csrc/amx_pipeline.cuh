@@ -624,10 +624,16 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
 
             if (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out)) {
                 uint64_t fl = 0;
+                if constexpr (B >= 8) {  // one multiplication per word (swar_gather_flags)
 #pragma unroll
-                for (int i = 0; i < SPT; i++)
+                    for (int i = 0; i < SPT; i++) fl |= (uint64_t)swar_gather_flags<B>(g[i]) << (i * EPS);
+                }
+                else {
 #pragma unroll
-                    for (int k = 0; k < EPS; k++) fl |= ((g[i] >> (k * B + B - 1)) & 1ull) << (i * EPS + k);
+                    for (int i = 0; i < SPT; i++)
+#pragma unroll
+                        for (int k = 0; k < EPS; k++) fl |= ((g[i] >> (k * B + B - 1)) & 1ull) << (i * EPS + k);
+                }
                 if (fl) {
                     const uint32_t wi = le0 >> 5, sh = le0 & 31;
                     atomicOr(&bitmap[wi], (uint32_t)(fl << sh));

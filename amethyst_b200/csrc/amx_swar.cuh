@@ -100,6 +100,29 @@ struct SwarPol {
     static_assert(!PLAIN || B <= 16, "the plain compressstore gathers 16-bit values");
 };
 
+// The E = floor(64/B) flags of a slab word (the top bit of each B-bit field of g, nothing else
+// set) gathered into bits 0..E-1 by one multiplication, for B >= 8.  With
+// M = sum_j 2^((E-1-j)(B-1)) the product term of field k and multiplier term j sits at bit
+// E(B-1) + k + (k-j)(B-1): j = k lands field k's flag at bit E(B-1) + k; k > j lands at or above
+// E(B-1) + E for B >= 9 (at B = 8 past bit 63); k < j lands below E(B-1), at distinct bits whose
+// sum stays below 2^(E(B-1)), so nothing carries into the window.  Terms past bit 63 drop out of
+// the 64-bit product without touching it.  tests/test_swar_cpu.py checks every pattern of every
+// width 8..32 (and that B = 7 fails).
+__host__ __device__ constexpr uint64_t swar_gather_mul(int b)
+{
+    uint64_t m = 0;
+    for (int j = 0; j < 64 / b; j++) m |= 1ull << ((64 / b - 1 - j) * (b - 1));
+    return m;
+}
+
+template <int B>
+__device__ __forceinline__ uint32_t swar_gather_flags(uint64_t g)
+{
+    static_assert(B >= 8 && B <= 32, "the single-product gather is exact for 8..32-bit fields");
+    constexpr int E = 64 / B;
+    return (uint32_t)((g * swar_gather_mul(B)) >> (E * (B - 1))) & ((1u << E) - 1);
+}
+
 // g[i] = in-place flags of word x[i] for the interval test selected by the template flags
 template <int B, int N, bool LO, bool HI, bool LOTOP, bool HITOP>
 __device__ __forceinline__ void swar_flags_t(const uint64_t (&x)[N], uint64_t (&g)[N], uint64_t l1, uint64_t l2)

@@ -130,6 +130,7 @@ WIDE_CASES = [
     # key fmt, key bits, val fmt, val bits, n, distinct keys (0: uniform over the key space)
     (SLAB, 32, SLAB, 16, 1 << 20, 1000),       # Zipf-weighted draws from 1000 random 32-bit keys
     (PLAIN32, 32, PLAIN32, 20, 300001, 0),     # nearly every key distinct: ~300K groups
+    (PLAIN32, 32, SLAB, 16, 1 << 20, 0),       # ~2^20 distinct groups
     (SLAB, 25, NOGAPS, 13, 400003, 0),         # ~4K collisions in a 25-bit space
     (NOGAPS, 28, SLAB, 7, 123457, 50000),
     (PLAIN64, 32, PLAIN64, 40, 77777, 3000),   # values wider than 32 bits
