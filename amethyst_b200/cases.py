@@ -15,6 +15,9 @@ larger than the 126 MB L2 unless the case says otherwise.
   groupby    2^26 Zipf(1.1) keys over 1000 groups at 10 bits, 2^26 u16 values at 16 bits
   groupby32  2^26 Zipf(1.1) keys drawn from 100,000 random 32-bit keys (32-bit slabs), 2^26 u16
              values: the wide-key hash table, the 512 MB key bitmap and the ordered extraction
+  mixed64    the 64 held-out operator chains of the mixed-chain bench line as one CUDA graph of
+             selector-planned programs (8 lanes); each timed replay runs inside the NVTX range
+             "mixed64-replay", so a profiler can list that replay's kernels alone
 """
 from __future__ import annotations
 
@@ -152,6 +155,33 @@ def case(name: str, reps: int = 10) -> dict:
         ms = _time(lambda: ops.groupby(keys, vals, ws=gws, max_groups=1 << 17), reps)
         ops.groupby_status(gws, 32)
         return {"case": name, "ms": ms, "GB_s": (keys.nbytes + vals.nbytes) / ms / 1e6}
+    if name == "mixed64":
+        from . import chains as X
+        from . import selector as S
+
+        rng = np.random.default_rng(99)
+        specs, k = [], 0
+        while len(specs) < 64:
+            ch = X.random_chain(rng, seed=100000 + k)
+            k += 1
+            if X.decision_points(ch):
+                specs.append(ch)
+        results = torch.zeros(sum(len(c.ops) for c in specs), dtype=torch.int64, device="cuda")
+        runners, slot = [], 0
+        for ch in specs:
+            runners.append(S.ChainRunner(ch, results, slot))
+            slot += len(ch.ops)
+        picks = S.Selector.load().choices(runners)
+        progs = [r.program(X.from_combo(p))[0] for r, p in zip(runners, picks)]
+        g = ops.Graph(progs, lanes=8)
+
+        def replay():
+            torch.cuda.nvtx.range_push("mixed64-replay")
+            g.launch()
+            torch.cuda.nvtx.range_pop()
+
+        ms = _time(replay, reps)
+        return {"case": name, "ms": ms, "elements": int(sum(c.n for c in specs))}
     raise ValueError(f"unknown case {name}")
 
 
