@@ -882,7 +882,8 @@ def main():
         dev = torch.device("cuda", 0)
         fn = {"mixed_chain": lambda d, k: mixed_chain(d, k, lanes=args.lanes), "batched_512": batched_512,
               "groupby_2e28": groupby_2e28, "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1,
-              "compressstore_masks": compressstore_masks}[args.only]
+              "compressstore_masks": compressstore_masks,
+              "fc_1gib": lambda d, k: fc_1gib(d, max(3, min(k, 30)), 3)}[args.only]
         print(json.dumps({args.only: fn(dev, args.steps)}), flush=True)
     else:
         run_gpu(args)
