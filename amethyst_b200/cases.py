@@ -11,6 +11,7 @@ larger than the 126 MB L2 unless the case says otherwise.
   fcB        filter v < 205 * 2^(B-11) + compressstore over 2^24 slabs of width B (e.g. fc11)
   filterB    filter -> bitmask over 2^24 slabs of width B
   matmul     4096^3 u7 x u7 slab matrices -> narrowest-width slabs (unpack + GEMM + pack)
+  matmul_fused  the same through the fused kernel (amx_tuning.policy 2)
   batch64    64 slab columns, lengths log-uniform in [2^16, 2^22], widths 1..32: one batch run
   groupby    2^26 Zipf(1.1) keys over 1000 groups at 10 bits, 2^26 u16 values at 16 bits
   groupby32  2^26 Zipf(1.1) keys drawn from 100,000 random 32-bit keys (32-bit slabs), 2^26 u16
@@ -100,8 +101,10 @@ def case(name: str, reps: int = 10) -> dict:
         ms = _time(step, reps)
         byts = col.nbytes + ops.storage_bytes(A.SLAB, bits, int(cnt[0].item())) + 8
         return {"case": name, "ms": ms, "GB_s": byts / ms / 1e6}
-    if name == "matmul":
+    if name in ("matmul", "matmul_fused"):
         M = N = K = 4096
+        if name == "matmul_fused":
+            A.check(L.amx_set_tuning(C.byref(A.Tuning(0, 0, 2, 0))))
 
         def slab_matrix(rows, cols, bits, seed):
             eps = 64 // bits

@@ -80,6 +80,35 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// Reads of a staged tile that the warp releases right after reading, before it is done with the
+// values: volatile, so the compiler can neither read the stage again later (when the loader may
+// already be refilling it) nor move the read past the release.  A packed-matrix kernel that read
+// its stage with plain loads and released it early got rows with data of the next slice when the
+// compiler re-read the stage after the release.
+__device__ __forceinline__ uint64_t lds_u64_v(const void* p)
+{
+    uint64_t v;
+    asm volatile("ld.volatile.shared.u64 %0, [%1];" : "=l"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint32_t lds_u32_v(const void* p)
+{
+    uint32_t v;
+    asm volatile("ld.volatile.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint4 lds_v4_v(const void* p)
+{
+    uint4 v;
+    asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"(smem_u32(p))
+                 : "memory");
+    return v;
+}
+
 // ---------------------------------------------------------------------------------------------
 // look-back status words: [63:62] flag, [61:0] value
 // ---------------------------------------------------------------------------------------------

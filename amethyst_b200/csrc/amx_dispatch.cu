@@ -94,7 +94,13 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
 
     const int id = choose_policy(p, force);
     if (id > kSwarPolicyBase) {
-        swar_setup(p);
+        if (p.has_pred) {
+            swar_setup(p);
+        }
+        else {  // an input mask alone: every field passes the (absent) predicate
+            p.sw_mode = 0;
+            p.sw_l1 = p.sw_l2 = 0;
+        }
         return launch_swar((uint32_t)(id - kSwarPolicyBase), p, ws, ws_bytes, stream);
     }
     // element-wise output with nothing else (conversions, binary ops): the runtime-format map

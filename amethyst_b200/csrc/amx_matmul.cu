@@ -6,12 +6,15 @@
 // src/common_code.cuh:124-129: row-major, every row padded to whole slabs) that the packed
 // operands and the packed result use here.
 //
-// Three steps, all stream-ordered:
+// Two paths.  The fused path (amx_mm_fused.cuh; slab operands of one width 1..8, selected with
+// amx_tuning.policy = 2 or 3): unpacker warps of the GEMM kernel turn the packed operands into
+// u8 tiles in its shared memory and the epilogue packs the product straight from the tensor
+// memory, so no operand or product is ever decompressed to HBM.  It unpacks every A slice once
+// per tile column and every B slice once per tile row (16x and 32x at 4096^3) on the ALU pipes,
+// and measured 1.5-2.3x slower than the two-pass path for K = 128..4096 at 4 and 7 bits, so the
+// automatic choice is the two-pass path here, three stream-ordered steps:
 //   1. mm_unpack_rows / mm_unpack_cols: the packed operands become u8 matrices in the workspace,
 //      A as M x K and B transposed to N x K (both K-major, rows padded to 128 bytes, padding 0).
-//      This costs one pass over 2 x 16 MB at 4096^3; unpacking inside the GEMM's shared memory
-//      instead would repeat it for every tile pair (32x for A, 16x for B at 128 x 256 tiles) on the
-//      ALU pipes that also feed the tensor cores.
 //   2. mm_gemm_kernel: persistent CTAs, one per SM, 128 x 256 output tiles.  One lane of warp 0
 //      streams 128-byte-deep K slices of A and B into a 4-stage shared-memory ring with 2-D TMA
 //      loads (128-byte swizzle, no multicast); one lane of warp 1 issues tcgen05.mma kind::i8
@@ -25,20 +28,9 @@
 #include <cudaTypedefs.h>
 
 #include "amx_dispatch.h"
-#include "amx_pipeline.cuh"
+#include "amx_mm_common.cuh"
 
 namespace amx {
-
-constexpr uint32_t kMmBM = 128;   // output rows per tile (TMEM lanes)
-constexpr uint32_t kMmBN = 256;   // output columns per tile (TMEM columns of one accumulator)
-constexpr uint32_t kMmBK = 128;   // K bytes per stage = one 128-byte swizzle row
-constexpr uint32_t kMmStages = 4;
-constexpr uint32_t kMmStageA = kMmBM * kMmBK;  // 16 KB
-constexpr uint32_t kMmStageB = kMmBN * kMmBK;  // 32 KB
-constexpr uint32_t kMmThreads = 192;           // TMA warp, MMA warp, 4 epilogue warps
-constexpr uint32_t kMmTmemCols = 2 * kMmBN;    // two accumulators
-constexpr uint32_t kMmSmem = 1024 + kMmStages * (kMmStageA + kMmStageB) + 256;
-constexpr uint32_t kMmMaxBits = 8;
 
 struct MmParams {
     uint32_t M, N, K;
@@ -46,60 +38,6 @@ struct MmParams {
     int32_t* c;  // M x N, row pitch N
     uint32_t* hdr;  // [0] largest entry, [1] error word
 };
-
-// ---------------------------------------------------------------------------------------------
-// tcgen05 / TMA building blocks (inline PTX)
-// ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int32_t x, int32_t y, uint64_t* bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 bytes apart
-__device__ __forceinline__ uint64_t sdesc_sw128(const void* p)
-{
-    const uint32_t a = smem_u32(p);
-    return (uint64_t)((a & 0x3FFFFu) >> 4) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
-           (2ull << 61);
-}
-
-__device__ __forceinline__ void umma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&r)[32])
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// instruction descriptor of kind::i8: D s32, A u8, B u8, both K-major, M = 128, N = 256
-constexpr uint32_t kMmIdesc = (2u << 4) | (0u << 7) | (0u << 10) | ((kMmBN >> 3) << 17) | ((kMmBM >> 4) << 24);
 
 // ---------------------------------------------------------------------------------------------
 // GEMM
@@ -438,8 +376,11 @@ __global__ void __launch_bounds__(256) mm_pack(const int32_t* c, uint32_t M, uin
 // ---------------------------------------------------------------------------------------------
 static uint64_t up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
+// Workspace: header, the fused path's column norms, u8 A and B^T of the two-pass path, and the
+// int32 product of the two-pass path (the fused path's repack scratch, up to 8 ceil(N/2) bytes a
+// row at widths of at most 31 bits).
 struct MmLayout {
-    uint64_t hdr, a8, b8, c32, total;
+    uint64_t hdr, colsq, a8, b8, c32, total;
     uint32_t kpad, mpad, npad;
 };
 
@@ -450,10 +391,11 @@ static MmLayout mm_layout(uint32_t M, uint32_t N, uint32_t K)
     l.mpad = (uint32_t)up(M ? M : 1, kMmBM);
     l.npad = (uint32_t)up(N ? N : 1, kMmBN);
     l.hdr = 0;
-    l.a8 = 1024;
+    l.colsq = 1024;
+    l.a8 = up(l.colsq + 8ull * l.npad, 1024);
     l.b8 = up(l.a8 + (uint64_t)l.mpad * l.kpad, 1024);
     l.c32 = up(l.b8 + (uint64_t)l.npad * l.kpad, 1024);
-    l.total = up(l.c32 + 4ull * M * N, 1024);
+    l.total = up(l.c32 + 4ull * M * N + 8ull * M + 16, 1024);
     return l;
 }
 
@@ -467,7 +409,7 @@ static uint32_t bit_length(uint64_t x)
     return b;
 }
 
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
@@ -565,6 +507,8 @@ amx_status amx_matmul(const amx_column* a, const amx_column* b, uint32_t M, uint
     if (e != cudaSuccess) return cuda_fail(e, "matmul: header clear");
     int32_t* c32 = reinterpret_cast<int32_t*>(w + L.c32);
     const uint64_t mn = (uint64_t)M * N;
+    if (mn && K && mf_applicable(a, b))  // unpacked in shared memory, packed from the accumulators
+        return mf_run(a, b, M, N, K, out, d_out_bits, hdr, reinterpret_cast<unsigned long long*>(w + L.colsq), c32, s);
     if (mn && K) {
         const ColDev ad = col_dev(a), bd = col_dev(b);
         const uint32_t chunks = L.kpad / 16;

@@ -115,6 +115,16 @@ __device__ __forceinline__ uint64_t bits_at(const uint32_t* w, uint32_t bit)
     return R == 64 ? x : (x & ((1ull << R) - 1));
 }
 
+// bits_at for a stage released right after the read (volatile reads)
+template <int R>
+__device__ __forceinline__ uint64_t bits_at_v(const uint32_t* w, uint32_t bit)
+{
+    const uint32_t wi = bit >> 5, sh = bit & 31;
+    uint64_t x = ((uint64_t)lds_u32_v(w + wi) | ((uint64_t)lds_u32_v(w + wi + 1) << 32)) >> sh;
+    if (R + sh > 64) x |= (uint64_t)lds_u32_v(w + wi + 2) << (64 - sh);
+    return R == 64 ? x : (x & ((1ull << R) - 1));
+}
+
 template <typename V>
 __device__ __forceinline__ V warp_incl_scan(V x)
 {
@@ -575,9 +585,9 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     uint64_t my_count = 0, my_agg = 0;
     uint32_t j = 0, s = 0, sphase = 0, q = 0, qphase = 0;
     if constexpr (Pol::kSwar) {
-        // Field-parallel path (one slab column, a predicate, no input mask): the flags are
-        // computed on whole slab words, the stage is released as soon as the thread's words are
-        // in registers, and only the passing fields are ever extracted.
+        // Field-parallel path (one slab column, a predicate and/or an input mask): the flags are
+        // computed on whole slab words, the stage is released as soon as the thread's words (and
+        // mask bits) are in registers, and only the passing fields are ever extracted.
         constexpr int B = Pol::kBits;
         constexpr int EPS = Pol::EPS;
         constexpr int SPT = Pol::SPT;
@@ -595,6 +605,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             const uint64_t rem = n - e0;
             const uint32_t valid = rem < TILE ? (uint32_t)rem : TILE;
             uint64_t x[SPT];
+            uint64_t mb = 0;  // the thread's R input-mask bits
             {
                 const uint8_t* st = stage0 + s * p.stage_bytes;
                 const uint64_t first = tile * (uint64_t)(T * SPT) + tid * SPT;  // first slab of this thread
@@ -603,12 +614,19 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     lds_words8_rot(src, x);  // tiles fall on 32 KB boundaries: 64-byte-aligned runs
                 else
                     lds_words<SPT>(src, x);
+                // tiles of T*R elements, T a multiple of 256: a tile's mask starts on a 32-byte
+                // boundary, the first staged byte
+                if (p.has_mask_in) mb = bits_at_v<R>(reinterpret_cast<const uint32_t*>(st + p.m_off), tid * R);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);  // the words are in registers: stage s is free
 
             uint64_t g[SPT];
             swar_flags<B, SPT>(p.sw_mode, x, g, p.sw_l1, p.sw_l2);
+            if (p.has_mask_in) {
+#pragma unroll
+                for (int i = 0; i < SPT; i++) g[i] &= swar_deposit_flags<B>(mb >> (i * EPS));
+            }
             const uint32_t le0 = tid * R;
             if (le0 + R > valid) {  // elements past the column's end do not pass
 #pragma unroll
@@ -746,7 +764,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             if (WM) {
                 uint64_t mfl = 0;
 #pragma unroll
-                for (int i = 0; i < R; i++) mfl |= (uint64_t)((mw[warp * R + i] >> lane) & 1u) << i;
+                for (int i = 0; i < R; i++) mfl |= (uint64_t)((lds_u32_v(mw + warp * R + i) >> lane) & 1u) << i;
                 fl &= mfl;
             }
             else {
@@ -1026,7 +1044,8 @@ __device__ __forceinline__ void finish_values(const PipeParams& p, V (&v)[R_], u
 
 // Warp-major reader with runtime format and width: lane `lane` of warp `warp` reads tile
 // elements warp*32R + 32i + lane, i = 0..R-1 (consecutive lanes hit consecutive or shared
-// words: no bank conflicts).
+// words: no bank conflicts).  Volatile reads: the warp-major policies release the stage right
+// after this.
 template <int R>
 __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* st, uint64_t sb, uint64_t e0,
                                                 uint64_t (&out)[R])
@@ -1038,13 +1057,13 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
         case AMX_PLAIN32: {
             const uint32_t* w = reinterpret_cast<const uint32_t*>(st) + (e0 - sb / 4) + base;
 #pragma unroll
-            for (int i = 0; i < R; i++) out[i] = w[32 * i] & m;
+            for (int i = 0; i < R; i++) out[i] = lds_u32_v(w + 32 * i) & m;
             break;
         }
         case AMX_PLAIN64: {
             const uint64_t* w = reinterpret_cast<const uint64_t*>(st) + (e0 - sb / 8) + base;
 #pragma unroll
-            for (int i = 0; i < R; i++) out[i] = w[32 * i] & m;
+            for (int i = 0; i < R; i++) out[i] = lds_u64_v(w + 32 * i) & m;
             break;
         }
         case AMX_SLAB: {
@@ -1057,7 +1076,7 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
                 const uint32_t x = r0 + base + 32 * i;
                 const uint32_t s = eps == 1 ? x : __umulhi(x, mg);
                 const uint32_t k = x - s * eps;
-                out[i] = (w[s] >> (k * b)) & m;
+                out[i] = (lds_u64_v(w + s) >> (k * b)) & m;
             }
             break;
         }
@@ -1069,7 +1088,7 @@ __device__ __forceinline__ void read_warp_major(const ColDev& c, const uint8_t* 
             for (int i = 0; i < R; i++) {
                 const uint64_t bp = bit0 + (uint64_t)(32 * i) * b;
                 const uint32_t wi = (uint32_t)(bp >> 6), off = (uint32_t)(bp & 63);
-                const uint64_t lo = w[wi], hi = w[wi + 1];
+                const uint64_t lo = lds_u64_v(w + wi), hi = lds_u64_v(w + wi + 1);
                 out[i] = (off ? ((lo >> off) | (hi << (64 - off))) : lo) & m;
             }
             break;

@@ -251,10 +251,10 @@ constexpr int kSwarPolicyBase = 200;
 #define AMX_PAIR(a, b) Slab2Pol<a, b>
 
 // A request the field-parallel slab policy (SwarPol) serves: one slab column of width <= 32, a
-// predicate on the field values themselves, no input mask, and a compacted output or none.
+// predicate on the field values themselves and/or an input mask, and a compacted output or none.
 inline bool swar_applicable(const PipeParams& p)
 {
-    return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && p.has_pred && !p.has_mask_in &&
+    return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && (p.has_pred || p.has_mask_in) &&
            (!p.has_out || p.compact) && p.op == AMX_OP_LHS && !p.need_vmask && p.vbits <= 32;
 }
 

@@ -21,7 +21,8 @@
 
 namespace amx {
 
-// load N consecutive 64-bit words from shared memory, 16 bytes at a time when aligned
+// load N consecutive 64-bit words from a stage released right after (volatile reads), 16 bytes
+// at a time when aligned
 template <int N>
 __device__ __forceinline__ void lds_words(const uint64_t* src, uint64_t (&w)[N])
 {
@@ -29,14 +30,14 @@ __device__ __forceinline__ void lds_words(const uint64_t* src, uint64_t (&w)[N])
         const uint4* s = reinterpret_cast<const uint4*>(src);
 #pragma unroll
         for (int i = 0; i < N / 2; i++) {
-            const uint4 x = s[i];
+            const uint4 x = lds_v4_v(s + i);
             w[2 * i] = ((uint64_t)x.y << 32) | x.x;
             w[2 * i + 1] = ((uint64_t)x.w << 32) | x.z;
         }
     }
     else {
 #pragma unroll
-        for (int i = 0; i < N; i++) w[i] = src[i];
+        for (int i = 0; i < N; i++) w[i] = lds_u64_v(src + i);
     }
 }
 
@@ -51,7 +52,7 @@ __device__ __forceinline__ void lds_words8_rot(const uint64_t* src, uint64_t (&w
     const uint4* s = reinterpret_cast<const uint4*>(src);
     uint4 t[4], u[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) t[k] = s[(k + r) & 3];  // t[k] = chunk (k + r) mod 4
+    for (int k = 0; k < 4; k++) t[k] = lds_v4_v(s + ((k + r) & 3));  // t[k] = chunk (k + r) mod 4
 #pragma unroll
     for (int c = 0; c < 4; c++) u[c] = (r & 1) ? t[(c + 3) & 3] : t[c];  // u[c] = t[c - (r & 1)]
 #pragma unroll
@@ -121,6 +122,39 @@ __device__ __forceinline__ uint32_t swar_gather_flags(uint64_t g)
     static_assert(B >= 8 && B <= 32, "the single-product gather is exact for 8..32-bit fields");
     constexpr int E = 64 / B;
     return (uint32_t)((g * swar_gather_mul(B)) >> (E * (B - 1))) & ((1u << E) - 1);
+}
+
+// The inverse of swar_gather_flags: bits 0..E-1 of m (E = floor(64/B)) placed on the top bits of
+// the E fields of a slab word, for an input mask.  A chunk of C <= B-1 flags times
+// D = sum_{j<C} 2^(j(B-1)) puts flag k at bit kB (term j = k); every other term (k != j, at bit
+// k + j(B-1)) falls on a bit that is no multiple of B and that no other term takes, since
+// |k - k'| < B - 1, so the product is a plain OR of shifted copies with no carries.  Chunks are
+// ORed in at offsets k0*B, and one shift and mask move bit kB to the field's top bit.  Bits of m
+// above E land past bit 63 or off the field tops.  One product per word for B >= 9, two for
+// B = 6..8, up to 32 for B = 2.  tests/test_swar_cpu.py checks every width against bit-by-bit
+// placement.
+__host__ __device__ constexpr uint64_t swar_deposit_mul(int b, int c)
+{
+    uint64_t d = 0;
+    for (int j = 0; j < c; j++) d |= 1ull << (j * (b - 1));
+    return d;
+}
+
+template <int B>
+__device__ __forceinline__ uint64_t swar_deposit_flags(uint64_t m)
+{
+    if constexpr (B == 1) {
+        return m;
+    }
+    else {
+        constexpr int E = 64 / B;
+        constexpr int C = (B - 1) < E ? (B - 1) : E;
+        constexpr uint64_t D = swar_deposit_mul(B, C);
+        uint64_t r = 0;
+#pragma unroll
+        for (int k0 = 0; k0 < E; k0 += C) r |= (((m >> k0) & ((1ull << C) - 1)) * D) << (k0 * B);
+        return (r << (B - 1)) & swar_top_bits(B);
+    }
 }
 
 // g[i] = in-place flags of word x[i] for the interval test selected by the template flags

@@ -362,7 +362,10 @@ def batched_512(dev, steps):
 def matmul_4096(dev, steps):
     """Dense 4096 x 4096 times 4096 x 4096 over unsigned 7-bit entries in slab rows (9 per slab,
     456 slabs per row), integer tensor cores with exact int32 accumulation, output packed at the
-    narrowest width holding the largest entry.  One step = unpack + GEMM + pack."""
+    narrowest width holding the largest entry.  One step = one amx_matmul call (the default
+    two-pass path: unpack, GEMM, pack); the fused kernel (amx_tuning.policy 2: unpack in shared
+    memory, pack from the accumulators) is timed beside it and its output compared byte for
+    byte."""
     import ctypes as C
 
     import torch
@@ -397,10 +400,25 @@ def matmul_4096(dev, steps):
     tot, _ = time_steps(step, reps, 3, torch.cuda.current_stream())
     ms = tot / reps
     A.check(L.amx_matmul_status(C.c_void_p(ws.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
-    res = {"workload": "4096^3 u7 x u7 slab matrices -> int32 -> narrowest-width slabs",
-           "ms_per_step": round(ms, 4), "TOPS": round(2 * M * N * K / (ms * 1e-3) / 1e12, 1),
-           "out_bits": int(width[0].item())}
-    del a, b, ws, out
+    bits = int(width[0].item())
+    nb = M * ((N + 64 // bits - 1) // (64 // bits)) * 8  # slab rows padded to whole words
+    two_pass = out.data[:nb].clone()
+    # the fused kernel (operands unpacked in shared memory from TMA-staged packed slices, the
+    # product packed from the tensor-memory accumulators), for comparison
+    A.check(L.amx_set_tuning(C.byref(A.Tuning(0, 0, 2, 0))))
+    try:
+        tot2, _ = time_steps(step, reps, 3, torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        same = bool(torch.equal(two_pass, out.data[:nb])) and int(width[0].item()) == bits
+    finally:
+        A.check(L.amx_set_tuning(None))
+    ms2 = tot2 / reps
+    res = {"workload": "4096^3 u7 x u7 slab matrices -> narrowest-width slabs; default: u8 operands unpacked once "
+                       "to the workspace, int32 product packed by a second pass",
+           "ms_per_step": round(ms, 4), "TOPS": round(2 * M * N * K / (ms * 1e-3) / 1e12, 1), "out_bits": bits,
+           "fused_ms": round(ms2, 4), "fused_TOPS": round(2 * M * N * K / (ms2 * 1e-3) / 1e12, 1),
+           "identical": same}
+    del a, b, ws, out, two_pass
     torch.cuda.empty_cache()
     return res
 

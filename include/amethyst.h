@@ -131,8 +131,11 @@ amx_status amx_workspace_status(const void* workspace, void* stream);
  * fields mean "automatic".  staged_bytes: input bytes kept staged ahead of the compute warps
  * (sets the depth of the shared-memory ring); compact_stages: ring depth of compacting passes;
  * policy: 0 automatic, 1 the generic runtime-width kernel, 1 + id a compile-time-width kernel
- * (id = slab width for one column); max_ctas: cap on the persistent grid of the group-by
- * aggregation (0: every CTA that fits).  amx_set_tuning(NULL) restores the defaults. */
+ * (id = slab width for one column); for amx_matmul 2 selects the fused kernel (operands unpacked
+ * in shared memory from TMA-staged packed slices, product packed from the accumulators; slab
+ * operands of one width) and 3 the same with the packed words read from global memory;
+ * max_ctas: cap on the persistent grid of the group-by aggregation (0: every CTA that fits).
+ * amx_set_tuning(NULL) restores the defaults. */
 typedef struct {
     uint32_t staged_bytes;
     uint32_t compact_stages;
@@ -274,8 +277,11 @@ amx_status amx_batch_status(const void* workspace, void* stream);
  * its largest entry and stores that width in *d_out_bits (device memory, may be NULL); size
  * `out` with amx_matmul_out_bytes(format, 0, ...), the widest possible case.  A nonzero
  * out->bits masks every entry to that width.  The workspace (amx_matmul_workspace_bytes) must be
- * 1024-byte aligned.  The reference has no matrix kernel, only the element accessors
- * (src/common_code.cuh:65-86,118-134). */
+ * 1024-byte aligned.  By default the operands are unpacked once to u8 in the workspace and the
+ * int32 product is packed by a second pass; amx_tuning.policy = 2 or 3 selects the fused kernel
+ * (slab operands of one width: unpacked in shared memory, packed from the accumulators, nothing
+ * decompressed to HBM), which is bit-identical and measured slower.  The reference has no matrix
+ * kernel, only the element accessors (src/common_code.cuh:65-86,118-134). */
 uint64_t amx_matmul_workspace_bytes(uint32_t M, uint32_t N, uint32_t K);
 uint64_t amx_matmul_out_bytes(uint32_t format, uint32_t out_bits, uint32_t M, uint32_t N, uint32_t K, uint32_t a_bits,
                               uint32_t b_bits);

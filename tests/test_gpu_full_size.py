@@ -222,7 +222,8 @@ def test_groupby_full_size(cuda):
 
 def test_matmul_full_size(cuda):
     """4096^3 u7 x u7 slab matrices: int32 output against an fp64 product (every entry is below
-    4096 * 127^2 < 2^53, so fp64 is exact), and the narrowest slab width of the output."""
+    4096 * 127^2 < 2^53, so fp64 is exact), a row block against the oracle, the narrowest slab
+    width of the output, and the fused kernel against both."""
     import torch
 
     from amethyst_b200 import ops
@@ -247,8 +248,27 @@ def test_matmul_full_size(cuda):
     ablk = O.matrix_encode(SLAB, 7, av[r0 * k:(r0 + rows) * k], rows, k)
     oc = O.matmul(ablk, SLAB, 7, braw, SLAB, 7, rows, n, k, threads=os.cpu_count() or 1)
     assert np.array_equal(got[r0:r0 + rows].cpu().numpy(), oc)
-    _, w = ops.matmul(a, b, m, n, k, out_fmt=SLAB, out_bits=0)
-    assert int(w[0].item()) == int(want.max().item()).bit_length()
+    o2, w = ops.matmul(a, b, m, n, k, out_fmt=SLAB, out_bits=0)
+    width = int(w[0].item())
+    assert width == int(want.max().item()).bit_length()
+    # the fused kernel (packed stages by TMA, 3-4 tiles per CTA), three runs: byte-identical to
+    # the two-pass output, the int32 product included (a stage released too early showed up only
+    # at this size, and not in every run)
+    import ctypes as C
+
+    from amethyst_b200 import _capi as A
+
+    nb = m * ((n + 64 // width - 1) // (64 // width)) * 8
+    try:
+        A.check(A.lib().amx_set_tuning(C.byref(A.Tuning(0, 0, 2, 0))))
+        for _ in range(3):
+            f32, _ = ops.matmul(a, b, m, n, k, out_fmt=PLAIN32, out_bits=32)
+            fs, fw = ops.matmul(a, b, m, n, k, out_fmt=SLAB, out_bits=0)
+            torch.cuda.synchronize()
+            assert torch.equal(f32.data[: 4 * m * n].view(torch.int32).long().reshape(m, n), got)
+            assert int(fw[0].item()) == width and torch.equal(fs.data[:nb], o2.data[:nb])
+    finally:
+        A.check(A.lib().amx_set_tuning(None))
 
 
 def test_batch_512_full_size(cuda):

@@ -1,6 +1,9 @@
 """The packed-integer matrix multiply (integer tensor cores) against the oracle's exact int64
 product, bit-exact, through the C ABI: every input format, ragged shapes that leave partial
-tiles in M, N and K, the narrowest-width output and fixed (masking) output widths."""
+tiles in M, N and K, the narrowest-width output and fixed (masking) output widths.  Slab
+operands of one width take the fused path (operands unpacked in shared memory, the product
+packed from the accumulators): every width 1..8, every output format, the repack when the
+precomputed packing width overshoots, and byte equality with the two-pass path."""
 import os
 
 import numpy as np
@@ -34,11 +37,11 @@ def dirty_slab_matrix(raw, bits, seed):
     return raw
 
 
-def check_case(m, n, k, af, ab, bf, bb, of, ob, seed):
+def check_case(m, n, k, af, ab, bf, bb, of, ob, seed, av=None, bv=None):
     from amethyst_b200 import ops
 
-    av = O.uniform_values(seed, ab, m * k)
-    bv = O.uniform_values(seed + 1, bb, k * n)
+    av = O.uniform_values(seed, ab, m * k) if av is None else av
+    bv = O.uniform_values(seed + 1, bb, k * n) if bv is None else bv
     araw = O.matrix_encode(af, ab, av, m, k)
     braw = O.matrix_encode(bf, bb, bv, k, n)
     if af == SLAB:
@@ -141,3 +144,92 @@ def test_matmul_repeated_and_status(cuda):
     torch.cuda.synchronize()
     assert torch.equal(r1, o2.data) and int(w1[0].item()) == int(w2[0].item())
     A.check(A.lib().amx_matmul_status(C.c_void_p(ws.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+
+@pytest.fixture
+def fused_policy(request):
+    """amx_tuning.policy 2 (the fused kernel, packed stages by TMA where the row pitches allow)
+    or 3 (the fused kernel reading the packed words from global memory) for the test."""
+    import ctypes as C
+
+    from amethyst_b200 import _capi as A
+
+    A.check(A.lib().amx_set_tuning(C.byref(A.Tuning(0, 0, request.param, 0))))
+    yield request.param
+    A.check(A.lib().amx_set_tuning(None))
+
+
+FUSED_CASES = [
+    # M, N, K, bits (both operands, slabs), out fmt, out bits
+    (128, 256, 128, 1, SLAB, 0),
+    (200, 300, 500, 2, NOGAPS, 0),
+    (129, 257, 385, 3, SLAB, 0),      # 21 fields per slab: every run residue, partial tiles
+    (256, 512, 640, 4, PLAIN32, 0),
+    (100, 1000, 300, 5, SLAB, 0),
+    (333, 517, 1000, 6, NOGAPS, 0),
+    (300, 600, 2048, 7, SLAB, 0),
+    (257, 255, 129, 8, PLAIN64, 0),
+    (128, 256, 256, 7, SLAB, 20),     # fixed narrower width: entries masked
+    (130, 260, 200, 5, NOGAPS, 13),
+    (64, 64, 64, 8, PLAIN32, 11),
+    (100, 300, 128, 7, SLAB, 40),     # fixed width above 32: one entry per slab
+    (1, 1, 1, 7, SLAB, 0),
+    (520, 270, 4096, 7, NOGAPS, 0),   # the matrix configuration's K, tile edges inside words
+    (384, 576, 1530, 7, SLAB, 0),     # even row pitches: packed stages by TMA
+    (333, 517, 1000, 6, NOGAPS, 0),
+    (256, 768, 1024, 3, PLAIN32, 0),
+]
+
+
+@pytest.mark.parametrize("fused_policy", [2, 3], indirect=True)
+@pytest.mark.parametrize("m,n,k,bits,of,ob", FUSED_CASES)
+def test_fused_matmul_matches_oracle(cuda, fused_policy, m, n, k, bits, of, ob):
+    check_case(m, n, k, SLAB, bits, SLAB, bits, of, ob, seed=m * 5 + n * 11 + k + bits)
+
+
+@pytest.mark.parametrize("fused_policy", [2], indirect=True)
+def test_fused_repack_when_the_bound_overshoots(cuda, fused_policy):
+    """A nonzero only in even columns and B's even rows only 0/1: the products stay small while
+    the row and column norms (the packing-width bound) are large, so the output is packed wide
+    and then repacked at the narrowest width.  Also the all-zero product (disjoint supports)."""
+    m, n, k, bits = 200, 300, 1024, 7
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 128, size=(m, k), dtype=np.uint64)
+    a[:, 1::2] = 0
+    b = rng.integers(0, 128, size=(k, n), dtype=np.uint64)
+    b[0::2, :] = rng.integers(0, 2, size=(k // 2, n), dtype=np.uint64)
+    for of in (SLAB, NOGAPS):
+        check_case(m, n, k, SLAB, bits, SLAB, bits, of, 0, seed=4, av=a.reshape(-1), bv=b.reshape(-1))
+    b[0::2, :] = 0
+    for of in (SLAB, NOGAPS, PLAIN32):
+        check_case(m, n, k, SLAB, bits, SLAB, bits, of, 0, seed=5, av=a.reshape(-1), bv=b.reshape(-1))
+
+
+def test_fused_and_two_pass_paths_agree(cuda):
+    """The same product through the fused kernel (amx_tuning.policy = 2, packed stages by TMA:
+    both row pitches are 170 and 72 words) and the default two-pass path is byte-identical, for a
+    slab and a nogaps output (K = 1530: the packing-width bound is one bit above the final width,
+    so the fused path also repacks here)."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    m, n, k = 384, 640, 1530
+    a = matrix_upload(O.matrix_encode(SLAB, 7, O.uniform_values(11, 7, m * k), m, k), m * k, SLAB, 7)
+    b = matrix_upload(O.matrix_encode(SLAB, 7, O.uniform_values(12, 7, k * n), k, n), k * n, SLAB, 7)
+    try:
+        for of in (SLAB, NOGAPS):
+            o2, w2 = ops.matmul(a, b, m, n, k, out_fmt=of)
+            A.check(A.lib().amx_set_tuning(C.byref(A.Tuning(0, 0, 2, 0))))
+            o1, w1 = ops.matmul(a, b, m, n, k, out_fmt=of)
+            A.check(A.lib().amx_set_tuning(None))
+            torch.cuda.synchronize()
+            width = int(w1[0].item())
+            assert width == int(w2[0].item())
+            nb = int(O.ora().ora_matrix_words(of, width, m, n)) * 8  # bytes past these are not output
+            assert torch.equal(o1.data[:nb], o2.data[:nb]), of
+    finally:
+        A.check(A.lib().amx_set_tuning(None))

@@ -125,3 +125,55 @@ def test_swar_count_and_aggregate_only(cuda, restore_tuning, bits, n):
             _, wcnt, wagg = O.chain(A.OP_LHS, (raw, SLAB, bits), None, bits, op, agg, None, None, n)
             assert int(cnt[0].item()) == wcnt, (bits, n, kind, agg)
             assert int(ag.cpu().numpy().view(np.uint64)[0]) == wagg, (bits, n, kind, agg)
+
+
+def _masks(n, seed):
+    """Input masks of n elements (LSB-first uint32 words, bits past n clear): random, none, all,
+    alternating, sparse, and runs that start and end inside words."""
+    rng = np.random.default_rng(seed)
+    words = (n + 31) // 32
+    runs = np.zeros(n, bool)
+    for a in rng.integers(0, max(n, 1), size=12):
+        runs[a : a + int(rng.integers(1, 5000))] = True
+    out = [
+        rng.integers(0, 2**32, size=words, dtype=np.uint64).astype(np.uint32),
+        np.zeros(words, np.uint32),
+        np.full(words, 0xFFFFFFFF, np.uint32),
+        np.full(words, 0xAAAAAAAA, np.uint32),
+        (rng.random(words) < 0.03).astype(np.uint32) * np.uint32(0x00010001),
+        np.packbits(np.concatenate([runs, np.zeros(words * 32 - n, bool)]), bitorder="little").view(np.uint32)
+        if words else np.zeros(0, np.uint32),
+    ]
+    for m in out:
+        if n % 32 and words:
+            m[-1] &= np.uint32((1 << (n % 32)) - 1)
+    return out
+
+
+@pytest.mark.parametrize("bits", list(range(1, 33)))
+def test_swar_mask_input(cuda, restore_tuning, bits):
+    """compressstore by a given mask (slabs at the input width: the plain variant up to 16 bits;
+    plain32 and nogaps: the general variant) and masked aggregates (the count-and-aggregate
+    variant), field-parallel policy forced and automatic, against the oracle bit-exact."""
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    n = [100003, 77777, 40961, (1 << 17) + 5][bits % 4]
+    v, raw = make_column(bits * 13 + 3, SLAB, bits, n)
+    col = to_gpu(raw, n, SLAB, bits)
+    words = (n + 31) // 32
+    for force in (1 + SWAR_BASE + bits, 0):
+        _set_policy(force)
+        for mi, m in enumerate(_masks(n, bits)):
+            dm = torch.zeros(words + 4, dtype=torch.int32, device="cuda")
+            dm[:words].copy_(torch.from_numpy(m.view(np.int32)))
+            for ofmt, obits in [(SLAB, bits), (A.PLAIN32, 32), (A.NOGAPS, bits)]:
+                out, cnt = ops.compressstore(col, dm, ofmt, obits)
+                want, wcnt = O.compressstore(raw, n, SLAB, bits, m, ofmt, obits)
+                assert int(cnt[0].item()) == wcnt, (bits, mi, ofmt)
+                assert np.array_equal(gpu_bytes(out, wcnt), want), (bits, mi, ofmt)
+            for agg in (A.AGG_SUM, A.AGG_MAX, A.AGG_XOR):
+                got = int(ops.reduce(agg, col, dm).cpu().numpy().view(np.uint64)[0])
+                assert got == O.reduce(agg, raw, n, SLAB, bits, m), (bits, mi, agg)
