@@ -93,6 +93,9 @@ _SIGS = {
     "amx_groupby_wide_workspace_bytes": (C.c_uint64, [C.c_uint32, C.c_uint64]),
     "amx_groupby_status": (C.c_int, [_P, C.c_uint32, _P]),
     "amx_groupby": (C.c_int, [_COL, _COL, _P, _COL, _COL, _COL, _P, _P, C.c_size_t, _P]),
+    "amx_groupby_sort_workspace_bytes": (C.c_uint64, [C.c_uint64, C.c_uint32, C.c_uint32]),
+    "amx_groupby_sort": (C.c_int, [_COL, _COL, _P, _COL, _COL, _COL, _P, _P, C.c_size_t, _P]),
+    "amx_groupby_sort_status": (C.c_int, [_P, _P]),
     "amx_matmul_workspace_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32]),
     "amx_matmul_out_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_uint32]),

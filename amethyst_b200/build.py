@@ -18,7 +18,7 @@ BUILD_DIR = os.path.join(ROOT, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
 
-UNITS = ["amx_capi.cu", "amx_dispatch.cu", "amx_swar.cu", "amx_swar_w0.cu", "amx_swar_w1.cu", "amx_swar_w2.cu", "amx_swar_w3.cu", "amx_datagen.cu", "amx_noalloc.cu", "amx_groupby.cu", "amx_matmul.cu", "amx_mm_fused.cu", "amx_mm_fused_w0.cu", "amx_mm_fused_w1.cu", "amx_batch.cu", "amx_selector.cu", "amx_pairs.cu", "amx_program.cu", "amx_stats.cu"]
+UNITS = ["amx_capi.cu", "amx_dispatch.cu", "amx_swar.cu", "amx_swar_w0.cu", "amx_swar_w1.cu", "amx_swar_w2.cu", "amx_swar_w3.cu", "amx_datagen.cu", "amx_noalloc.cu", "amx_groupby.cu", "amx_groupby_sort.cu", "amx_matmul.cu", "amx_mm_fused.cu", "amx_mm_fused_w0.cu", "amx_mm_fused_w1.cu", "amx_batch.cu", "amx_selector.cu", "amx_pairs.cu", "amx_program.cu", "amx_stats.cu"]
 
 
 def _sources():

@@ -16,6 +16,7 @@ larger than the 126 MB L2 unless the case says otherwise.
   groupby    2^26 Zipf(1.1) keys over 1000 groups at 10 bits, 2^26 u16 values at 16 bits
   groupby32  2^26 Zipf(1.1) keys drawn from 100,000 random 32-bit keys (32-bit slabs), 2^26 u16
              values: the wide-key hash table, the 512 MB key bitmap and the ordered extraction
+  groupby32_sort  the same through the sort-based group-by (radix sort + reduce-by-key)
   mixed64    the 64 held-out operator chains of the mixed-chain bench line as one CUDA graph of
              selector-planned programs (8 lanes); each timed replay runs inside the NVTX range
              "mixed64-replay", so a profiler can list that replay's kernels alone
@@ -147,16 +148,21 @@ def case(name: str, reps: int = 10) -> dict:
         gws = gws[(-gws.data_ptr()) % 256:]
         ms = _time(lambda: ops.groupby(keys, vals, ws=gws), reps)
         return {"case": name, "ms": ms, "GB_s": (keys.nbytes + vals.nbytes) / ms / 1e6}
-    if name == "groupby32":
+    if name in ("groupby32", "groupby32_sort"):
         n, groups = 1 << 26, 100000
         idx, _ = datagen.keys_from_cdf_gpu(n, datagen.zipf_cdf(groups, 1.1), 5)
         pool = torch.from_numpy(np.random.default_rng(6).choice(1 << 32, size=groups, replace=False)).cuda()
         k32 = pool[idx[:n].long()].to(torch.int64).bitwise_and(0xFFFFFFFF).to(torch.int32)
         keys = ops.convert(ops.PackedColumn(k32.contiguous().view(torch.uint8), n, A.PLAIN32, 32), A.SLAB, 32)
         vals = _gen(n, 16, 7)
-        gws = ops.groupby_workspace(32, 1 << 17)
-        ms = _time(lambda: ops.groupby(keys, vals, ws=gws, max_groups=1 << 17), reps)
-        ops.groupby_status(gws, 32)
+        if name == "groupby32_sort":
+            sws = ops.aligned_bytes(int(L.amx_groupby_sort_workspace_bytes(n, 32, 16)), 256)
+            ms = _time(lambda: ops.groupby_sort(keys, vals, ws=sws, max_groups=1 << 17), reps)
+            A.check(L.amx_groupby_sort_status(C.c_void_p(sws.data_ptr()), s))
+        else:
+            gws = ops.groupby_workspace(32, 1 << 17)
+            ms = _time(lambda: ops.groupby(keys, vals, ws=gws, max_groups=1 << 17), reps)
+            ops.groupby_status(gws, 32)
         return {"case": name, "ms": ms, "GB_s": (keys.nbytes + vals.nbytes) / ms / 1e6}
     if name == "mixed64":
         from . import chains as X

@@ -471,6 +471,72 @@ def fc_cfg1(dev, steps):
             "alg_bytes": byts}
 
 
+def groupby_wide(dev, steps):
+    """Group-by with 32-bit keys, hash tables (amx_groupby) against radix sort + reduce-by-key
+    (amx_groupby_sort), 2^26 keys in 32-bit slabs and 2^26 u16 values in 16-bit slabs: Zipf(1.1)
+    draws from 100,000 random keys; uniform draws from 2^20 and from 2^23 random keys; uniform
+    32-bit keys (about 2^26 distinct groups).  The two outputs are compared byte for byte."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import datagen, ops
+
+    n = 1 << 26
+    L = A.lib()
+    vals = pack_gpu(n, 16, 0x7A2, 2)
+    rows = {}
+    for name in ("zipf_100k_keys", "uniform_from_1m_keys", "uniform_from_8m_keys", "uniform_32bit_keys"):
+        if name == "zipf_100k_keys":
+            idx, _ = datagen.keys_from_cdf_gpu(n, datagen.zipf_cdf(100000, 1.1), 5)
+            pool = torch.from_numpy(np.random.default_rng(6).choice(1 << 32, size=100000, replace=False)).to(dev)
+            k32 = pool[idx[:n].long()].bitwise_and(0xFFFFFFFF).to(torch.int32)
+            del idx, pool
+            cap = 1 << 17
+        elif name.startswith("uniform_from"):
+            m = (1 << 20) if "1m" in name else (1 << 23)
+            pool = torch.from_numpy(np.random.default_rng(7).choice(1 << 32, size=m, replace=False)).to(dev)
+            idx = datagen.uniform_gpu(n, 32, 0x5EEE + m).long().bitwise_and(0xFFFFFFFF) % m
+            k32 = pool[idx[:n]].bitwise_and(0xFFFFFFFF).to(torch.int32)
+            del idx, pool
+            cap = m
+        else:
+            k32 = datagen.uniform_gpu(n, 32, 0x5EED)
+            cap = n
+        keys = ops.convert(ops.PackedColumn(k32.contiguous().view(torch.uint8), n, A.PLAIN32, 32), A.SLAB, 32)
+        del k32
+        torch.cuda.empty_cache()
+        reps = max(3, min(steps, 10))
+        gws = ops.groupby_workspace(32, cap)
+        res = {}
+        tot, _ = time_steps(lambda: res.__setitem__("h", ops.groupby(keys, vals, ws=gws, max_groups=cap)), reps, 3,
+                            torch.cuda.current_stream())
+        ms_h = tot / reps
+        ops.groupby_status(gws, 32)
+        del gws
+        torch.cuda.empty_cache()
+        sws = ops.aligned_bytes(int(L.amx_groupby_sort_workspace_bytes(n, 32, 16)), 256)
+        tot, _ = time_steps(lambda: res.__setitem__("s", ops.groupby_sort(keys, vals, ws=sws, max_groups=cap)), reps,
+                            3, torch.cuda.current_stream())
+        ms_s = tot / reps
+        A.check(L.amx_groupby_sort_status(C.c_void_p(sws.data_ptr()),
+                                          C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        g = int(res["h"][3][0].item())
+        same = g == int(res["s"][3][0].item())
+        for x, y in zip(res["h"][:3], res["s"][:3]):
+            nb = storage_bytes(x.fmt, x.bits, g)
+            same = same and bool(torch.equal(x.data[:nb], y.data[:nb]))
+        rows[name] = {"groups": g, "hash_ms": round(ms_h, 4), "sort_ms": round(ms_s, 4), "identical": same}
+        del keys, sws, res
+        torch.cuda.empty_cache()
+    del vals
+    torch.cuda.empty_cache()
+    return {"workload": "group-by sum+count, 2^26 32-bit keys (32-bit slabs) + u16 values: hash tables vs radix "
+                        "sort + reduce-by-key", "rows": rows}
+
+
 def groupby_2e28(dev, steps):
     """Group-by at 1 GB: 2^28 keys Zipf(s=1.1) over 1000 groups packed at 10 bits, 2^28 values
     uniform in [0, 2^16) packed at 16 bits; per-group uint64 sum and count."""
@@ -802,6 +868,10 @@ def run_gpu(args):
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["groupby_2e28"] = {"error": str(e)}
             try:
+                extra["groupby_wide"] = groupby_wide(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["groupby_wide"] = {"error": str(e)}
+            try:
                 extra["matmul_4096"] = matmul_4096(dev, args.steps)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["matmul_4096"] = {"error": str(e)}
@@ -899,7 +969,7 @@ def main():
         torch.cuda.set_device(0)
         dev = torch.device("cuda", 0)
         fn = {"mixed_chain": lambda d, k: mixed_chain(d, k, lanes=args.lanes), "batched_512": batched_512,
-              "groupby_2e28": groupby_2e28, "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1,
+              "groupby_2e28": groupby_2e28, "groupby_wide": groupby_wide, "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1,
               "compressstore_masks": compressstore_masks,
               "fc_1gib": lambda d, k: fc_1gib(d, max(3, min(k, 30)), 3)}[args.only]
         print(json.dumps({args.only: fn(dev, args.steps)}), flush=True)

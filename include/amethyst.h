@@ -230,6 +230,22 @@ amx_status amx_groupby(const amx_column* keys, const amx_column* vals, const uin
                        const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
                        uint64_t* d_groups, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Sort-based group-by: the same results as amx_groupby (ascending keys, uint64 sums, counts) for
+ * keys of 1..32 bits and values of 1..64 bits in any format, by an LSD radix sort of the key/value
+ * pairs in 8-bit digits followed by a reduce-by-key -- the reference's sort path
+ * (src/benchs/bench_groupby_sort_cub.cu:48-66: cub::DeviceRadixSort::SortPairs then
+ * cub::DeviceReduce::ReduceByKey).  Its cost does not depend on the number of groups, which has
+ * no bound but n.  Outputs hold as many groups as their capacity; more groups record
+ * AMX_ERR_CAPACITY (amx_groupby_sort_status).  The workspace (256-byte aligned) holds two copies
+ * of the pairs and one of the groups: amx_groupby_sort_workspace_bytes(n, key_bits, value_bits). */
+uint64_t amx_groupby_sort_workspace_bytes(uint64_t n, uint32_t key_bits, uint32_t value_bits);
+amx_status amx_groupby_sort(const amx_column* keys, const amx_column* vals, const uint32_t* d_mask,
+                            const amx_column* out_keys, const amx_column* out_sums, const amx_column* out_counts,
+                            uint64_t* d_groups, void* workspace, size_t workspace_bytes, void* stream);
+/* synchronises `stream`, then reports a device-side failure recorded by the last amx_groupby_sort
+ * that used `workspace` */
+amx_status amx_groupby_sort_status(const void* workspace, void* stream);
+
 /* ---- batches of columns ------------------------------------------------------------------ */
 /* Filter + compressstore + sum over `ncols` slab columns of any lengths and widths (1..32 bits)
  * in one persistent launch.  Column i keeps the elements that pass preds[i], compacted into

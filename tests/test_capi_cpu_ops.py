@@ -137,3 +137,30 @@ def test_noalloc_rejects_oversized_columns_before_any_device_work(lib):
     pred = A.Predicate(A.PRED_LT, 11, 205, 0)
     assert lib.amx_filter_compressstore_noalloc(C.byref(big), C.byref(pred), C.byref(out), None, None) == 7
     assert b"2^29" in lib.amx_last_error()
+
+
+def test_groupby_sort_sizing_and_errors(lib):
+    """amx_groupby_sort: workspace sizes (two copies of the pairs, one of the groups) and the
+    argument checks that return before any device work."""
+    from amethyst_b200 import _capi as A
+
+    assert lib.amx_groupby_sort_workspace_bytes(1000, 0, 16) == 0
+    assert lib.amx_groupby_sort_workspace_bytes(1000, 33, 16) == 0
+    assert lib.amx_groupby_sort_workspace_bytes(1000, 32, 65) == 0
+    w32 = lib.amx_groupby_sort_workspace_bytes(1 << 20, 32, 16)
+    w64 = lib.amx_groupby_sort_workspace_bytes(1 << 20, 32, 40)
+    assert w32 % 256 == 0 and w32 >= (1 << 20) * (2 * 4 + 2 * 4 + 4 + 8 + 8)
+    assert w64 >= w32 + (1 << 20) * 8  # 64-bit values carried for values over 32 bits
+    assert lib.amx_groupby_sort_workspace_bytes(0, 10, 10) > 0
+    keys = col(0x100000, 100, A.SLAB, 10)
+    vals = col(0x200000, 100, A.SLAB, 16)
+    out = col(0x300000, 100, A.PLAIN64, 64)
+    g = C.c_void_p(0x500000)
+    w = lib.amx_groupby_sort_workspace_bytes(100, 10, 16)
+    call = lambda k, v, ws, wb: lib.amx_groupby_sort(C.byref(k), C.byref(v), None, C.byref(out), C.byref(out),  # noqa: E731
+                                                     C.byref(out), g, ws, wb, None)
+    assert call(col(0x100000, 100, A.SLAB, 33), vals, C.c_void_p(0x400000), 1 << 30) == 2  # keys over 32 bits
+    assert call(keys, col(0x200000, 99, A.SLAB, 16), C.c_void_p(0x400000), w) == 1       # lengths differ
+    assert call(keys, vals, C.c_void_p(0x400000), w - 1) == 4                            # workspace too small
+    assert call(keys, vals, C.c_void_p(0x400010), w) == 3                                # not 256-byte aligned
+    assert lib.amx_groupby_sort_status(None, None) == 1
