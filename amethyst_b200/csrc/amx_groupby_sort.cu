@@ -18,8 +18,9 @@
 //                           addresses;
 //   3. reduce-by-key over the sorted pairs: gs_heads_kernel counts the first pair of every key
 //      run per tile, gs_scan_heads_kernel turns the counts into group numbers (and writes the
-//      group count), and gs_reduce_kernel sums each run with warp-segmented reductions; runs that
-//      cross a tile boundary are added with global atomics, all others stored;
+//      group count), and gs_reduce_kernel sums each run as the difference of two running sums of
+//      a block scan; runs that cross a tile boundary are added with global atomics, all others
+//      stored;
 //   4. the tile pipeline encodes keys, sums and counts into the caller's columns, reading the
 //      group count on the device.
 // The cost is independent of the number of groups: about 20 bytes per pair and pass moved
@@ -156,7 +157,7 @@ __device__ __forceinline__ uint32_t gs_block_excl256(uint32_t v, uint32_t* wsum)
 
 // One LSD pass: every pair of the tile to its place in the output, stable.
 template <typename V>
-__global__ void __launch_bounds__(kGsThreads, 2) gs_scatter_kernel(const uint32_t* kin, const V* vin, uint32_t* kout,
+__global__ void __launch_bounds__(kGsThreads, 4) gs_scatter_kernel(const uint32_t* kin, const V* vin, uint32_t* kout,
                                                                 V* vout, uint64_t n_max, const uint64_t* n_dev,
                                                                 uint32_t shift, const uint32_t* counts, uint64_t tiles,
                                                                 const uint32_t* tot)
@@ -181,14 +182,18 @@ __global__ void __launch_bounds__(kGsThreads, 2) gs_scatter_kernel(const uint32_
     gbase[tid] = (uint64_t)dbase + counts[(uint64_t)tid * tiles + tile];
     __syncthreads();
 
+    // only the ranks stay in registers between the phases (keys and values are read again below:
+    // cache hits), so more CTAs fit per SM
     uint32_t key[kGsPer], rank[kGsPer];
-    V val[kGsPer];
+#pragma unroll
+    for (uint32_t i = 0; i < kGsPer; i++) {
+        const uint32_t s = gs_slot(w, i, lane);
+        key[i] = s < valid ? kin[e0 + s] : 0u;
+    }
 #pragma unroll
     for (uint32_t i = 0; i < kGsPer; i++) {
         const uint32_t s = gs_slot(w, i, lane);
         const bool ok = s < valid;
-        key[i] = ok ? kin[e0 + s] : 0u;
-        val[i] = ok ? vin[e0 + s] : (V)0;
         const uint32_t d = (key[i] >> shift) & 255u;
         const uint32_t peers = gs_peers(d, ok);
         const uint32_t below = (uint32_t)__popc(peers & ((1u << lane) - 1));
@@ -209,14 +214,15 @@ __global__ void __launch_bounds__(kGsThreads, 2) gs_scatter_kernel(const uint32_
     }
     dstart[tid] = gs_block_excl256(tcount, wsum);
     __syncthreads();
-#pragma unroll
+#pragma unroll 4
     for (uint32_t i = 0; i < kGsPer; i++) {
         const uint32_t s = gs_slot(w, i, lane);
         if (s < valid) {
-            const uint32_t d = (key[i] >> shift) & 255u;
+            const uint32_t k = kin[e0 + s];
+            const uint32_t d = (k >> shift) & 255u;
             const uint32_t pos = dstart[d] + wcnt[w][d] + rank[i];
-            sk[pos] = key[i];
-            sv[pos] = val[i];
+            sk[pos] = k;
+            sv[pos] = vin[e0 + s];
         }
     }
     __syncthreads();
@@ -297,106 +303,160 @@ __global__ void __launch_bounds__(1024) gs_scan_heads_kernel(const uint32_t* til
     if (tid == 0) *d_groups = carry;
 }
 
-// Sums and counts of the key runs.  Group g of a pair = the tile's first group number + the
-// heads up to it inside the tile - 1.  Each warp reduces the runs of its 32 consecutive pairs per
-// round (segmented shuffle sums) into shared partials; a tile's runs that start and end inside
-// it are stored, the first (continuing from the tile before) and the last (continuing into the
-// next) are added with atomics into the zeroed outputs.
+// Sums and counts of the key runs.  Thread t takes pairs 16t .. 16t+15 of the tile; a block scan
+// of the head counts numbers the runs (group g = the tile's first group number + the heads up to
+// the pair - 1; run 0 is the one continuing from the tile before) and a block scan of the values
+// gives every pair's running sum.  The thread holding a run's first pair records the running sum
+// before it and its position; the thread holding its last pair turns them into the run's sum and
+// length.  Runs that start and end inside the tile are stored, the first (continuing from the tile
+// before) and the last (continuing into the next) are added with atomics into the zeroed outputs.
 template <typename V>
 __global__ void __launch_bounds__(kGsThreads) gs_reduce_kernel(const uint32_t* keys, const V* vals, uint64_t n_max,
                                                                const uint64_t* n_dev, const uint64_t* seg_base,
                                                                uint32_t* okey, unsigned long long* osum,
                                                                unsigned long long* ocnt, uint64_t cap, uint32_t* err)
 {
-    extern __shared__ uint4 gs_dyn[];  // per run of the tile: partial sum, then partial count
-    unsigned long long* psum = reinterpret_cast<unsigned long long*>(gs_dyn);
-    uint32_t* pcnt = reinterpret_cast<uint32_t*>(psum + kGsTile + 1);
-    __shared__ uint32_t wheads[kGsWarps][kGsPer];
+    extern __shared__ uint4 gs_dyn[];  // per run: running sum before its first pair, then that position
+    unsigned long long* rstart = reinterpret_cast<unsigned long long*>(gs_dyn);
+    uint32_t* pstart = reinterpret_cast<uint32_t*>(rstart + kGsTile + 1);
+    __shared__ uint32_t wh[kGsWarps];
+    __shared__ unsigned long long wv[kGsWarps];
     const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const uint64_t tile = blockIdx.x;
     const uint64_t n = gs_len(n_max, n_dev);
     const uint64_t e0 = tile * kGsTile;
     if (e0 >= n) return;
     const uint32_t valid = n - e0 < kGsTile ? (uint32_t)(n - e0) : kGsTile;
-    for (uint32_t i = tid; i <= kGsTile; i += kGsThreads) {
-        psum[i] = 0;
-        pcnt[i] = 0;
-    }
-    // head flags per round: ballots, and each round's head count
-    uint32_t hb[kGsPer];
+    const uint32_t b = tid * kGsPer;
+    uint32_t k[kGsPer];
+    unsigned long long v[kGsPer];
+    if (b + kGsPer <= valid) {  // 16-byte loads: the buffers and the caller's columns are 16-byte aligned
+        const uint4* kq = reinterpret_cast<const uint4*>(keys + e0 + b);
 #pragma unroll
-    for (uint32_t i = 0; i < kGsPer; i++) {
-        const uint32_t s = gs_slot(w, i, lane);
-        hb[i] = __ballot_sync(0xffffffffu, s < valid && gs_head(keys, e0 + s));
-        if (lane == 0) wheads[w][i] = (uint32_t)__popc(hb[i]);
-    }
-    __syncthreads();
-    // heads before each (warp, round) in tile order: warps in order, rounds in order
-    uint32_t before = 0;
-    for (uint32_t k = 0; k < w; k++)
-        for (uint32_t i = 0; i < kGsPer; i++) before += wheads[k][i];
-    const uint32_t total_heads = [&] {
-        uint32_t t = 0;
-        for (uint32_t k = 0; k < kGsWarps; k++)
-            for (uint32_t i = 0; i < kGsPer; i++) t += wheads[k][i];
-        return t;
-    }();
-    uint32_t locs[kGsPer];
+        for (uint32_t q = 0; q < kGsPer / 4; q++) {
+            const uint4 x = kq[q];
+            k[4 * q] = x.x;
+            k[4 * q + 1] = x.y;
+            k[4 * q + 2] = x.z;
+            k[4 * q + 3] = x.w;
+        }
+        const uint4* vq = reinterpret_cast<const uint4*>(vals + e0 + b);
+        if constexpr (sizeof(V) == 4) {
 #pragma unroll
-    for (uint32_t i = 0; i < kGsPer; i++) {
-        const uint32_t s = gs_slot(w, i, lane);
-        const bool ok = s < valid;
-        // local run index: heads up to this pair inside the tile (0 = the run continuing from
-        // the tile before)
-        const uint32_t loc = before + (uint32_t)__popc(hb[i] & (0xffffffffu >> (31 - lane)));
-        locs[i] = loc;
-        before += (uint32_t)__popc(hb[i]);
-        unsigned long long v = ok ? (unsigned long long)vals[e0 + s] : 0ull;
-        // segmented sum toward the first lane of each run in this round: lane + o belongs to this
-        // lane's run when no head lies in (lane, lane + o]
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long yv = __shfl_down_sync(0xffffffffu, v, o);
-            const uint32_t span = lane + o < 32 ? (((2u << (lane + o)) - 1) & ~((2u << lane) - 1)) : 0u;
-            if (lane + o < 32 && (hb[i] & span) == 0) v += yv;
-        }
-        // the first lane of each run in this round adds the run's sum and length
-        if (ok && (lane == 0 || ((hb[i] >> lane) & 1))) {
-            const uint32_t later = hb[i] & ~((2u << lane) - 1);  // heads after this lane
-            const uint32_t end = later ? (uint32_t)(__ffs(later) - 1) : 32u;
-            const uint32_t lim = valid > i * 32 + w * (32 * kGsPer) ? valid - (i * 32 + w * (32 * kGsPer)) : 0u;
-            const uint32_t c = (end < lim ? end : lim) - lane;
-            atomicAdd(&psum[loc], v);
-            atomicAdd(&pcnt[loc], c);
-        }
-    }
-    __syncthreads();
-    // does the tile's last run continue into the next tile?
-    const bool open_end = valid == kGsTile && e0 + kGsTile < n && keys[e0 + kGsTile] == keys[e0 + kGsTile - 1];
-    const uint64_t g0 = seg_base[tile];  // group number of the tile's first head
-    for (uint32_t loc = tid; loc <= total_heads; loc += kGsThreads) {
-        if (pcnt[loc] == 0) continue;  // no continuing run (the tile starts with a head)
-        const uint64_t g = g0 + loc - 1;  // loc 0: the run that began before this tile
-        if (g >= cap) {
-            record_error(err, AMX_ERR_CAPACITY);
-            continue;
-        }
-        if (loc == 0 || (loc == total_heads && open_end)) {
-            atomicAdd(&osum[g], psum[loc]);
-            atomicAdd(&ocnt[g], (unsigned long long)pcnt[loc]);
+            for (uint32_t q = 0; q < kGsPer / 4; q++) {
+                const uint4 x = vq[q];
+                v[4 * q] = x.x;
+                v[4 * q + 1] = x.y;
+                v[4 * q + 2] = x.z;
+                v[4 * q + 3] = x.w;
+            }
         }
         else {
-            osum[g] = psum[loc];
-            ocnt[g] = pcnt[loc];
+#pragma unroll
+            for (uint32_t q = 0; q < kGsPer / 2; q++) {
+                const uint4 x = vq[q];
+                v[2 * q] = ((unsigned long long)x.y << 32) | x.x;
+                v[2 * q + 1] = ((unsigned long long)x.w << 32) | x.z;
+            }
         }
     }
-    // group keys, written by each head
+    else {
 #pragma unroll
-    for (uint32_t i = 0; i < kGsPer; i++) {
-        const uint32_t s = gs_slot(w, i, lane);
-        if ((hb[i] >> lane) & 1) {
-            const uint64_t g = g0 + locs[i] - 1;
-            if (g < cap) okey[g] = keys[e0 + s];
+        for (uint32_t j = 0; j < kGsPer; j++) {
+            const bool ok = b + j < valid;
+            k[j] = ok ? keys[e0 + b + j] : 0u;
+            v[j] = ok ? (unsigned long long)vals[e0 + b + j] : 0ull;
+        }
+    }
+    const bool has_prev = e0 + b > 0 && b < valid;
+    const uint32_t kprev = has_prev ? keys[e0 + b - 1] : 0u;
+    const bool has_next = b + kGsPer < valid || (b + kGsPer == kGsTile && e0 + kGsTile < n);
+    const uint32_t knext = has_next ? keys[e0 + b + kGsPer] : 0u;
+    uint32_t hf = 0;  // bit j: pair j starts a run
+    unsigned long long vs = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < kGsPer; j++) {
+        const bool ok = b + j < valid;
+        const bool head = ok && (j ? k[j] != k[j - 1] : (!has_prev || k[0] != kprev));
+        hf |= (head ? 1u : 0u) << j;
+        vs += v[j];
+    }
+    // block scans: heads and values before this thread
+    uint32_t hx = (uint32_t)__popc(hf);
+    unsigned long long vx = vs;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t yh = __shfl_up_sync(0xffffffffu, hx, o);
+        const unsigned long long yv = __shfl_up_sync(0xffffffffu, vx, o);
+        if (lane >= (uint32_t)o) {
+            hx += yh;
+            vx += yv;
+        }
+    }
+    if (lane == 31) {
+        wh[w] = hx;
+        wv[w] = vx;
+    }
+    __syncthreads();
+    uint32_t hbefore = hx - (uint32_t)__popc(hf), total_heads = 0;
+    unsigned long long vbefore = vx - vs;
+    for (uint32_t q = 0; q < kGsWarps; q++) {
+        if (q < w) {
+            hbefore += wh[q];
+            vbefore += wv[q];
+        }
+        total_heads += wh[q];
+    }
+    if (tid == 0 && !(hf & 1u)) {  // the run continuing from the tile before
+        rstart[0] = 0;
+        pstart[0] = 0;
+    }
+    // run starts
+    {
+        uint32_t loc = hbefore;
+        unsigned long long run = vbefore;
+#pragma unroll
+        for (uint32_t j = 0; j < kGsPer; j++) {
+            if ((hf >> j) & 1u) {
+                loc++;
+                rstart[loc] = run;
+                pstart[loc] = b + j;
+            }
+            run += v[j];
+        }
+    }
+    __syncthreads();
+    // run ends: the last valid pair of the tile, or a pair followed by a head
+    const bool open_end = valid == kGsTile && e0 + kGsTile < n && keys[e0 + kGsTile] == keys[e0 + kGsTile - 1];
+    const uint64_t g0 = seg_base[tile];  // group number of the tile's first head
+    uint32_t loc = hbefore;
+    unsigned long long run = vbefore;
+#pragma unroll
+    for (uint32_t j = 0; j < kGsPer; j++) {
+        const bool ok = b + j < valid;
+        if ((hf >> j) & 1u) {
+            loc++;
+            const uint64_t g = g0 + loc - 1;
+            if (g < cap) okey[g] = k[j];
+        }
+        run += v[j];
+        const bool last = b + j + 1 == valid;
+        const bool next_head = j + 1 < kGsPer ? ((hf >> (j + 1)) & 1u) != 0 : (has_next && knext != k[j]);
+        if (ok && (last || next_head)) {
+            const unsigned long long sum = run - rstart[loc];
+            const unsigned long long cnt = (unsigned long long)(b + j + 1 - pstart[loc]);
+            const uint64_t g = g0 + loc - 1;  // loc 0: the run that began before this tile
+            if (g >= cap) {
+                record_error(err, AMX_ERR_CAPACITY);
+            }
+            else if (loc == 0 || (loc == total_heads && last && open_end)) {
+                atomicAdd(&osum[g], sum);
+                atomicAdd(&ocnt[g], cnt);
+            }
+            else {
+                osum[g] = sum;
+                ocnt[g] = cnt;
+            }
         }
     }
 }
@@ -519,7 +579,7 @@ amx_status groupby_sort_run(const amx_column* keys, const amx_column* vals, cons
     uint32_t* tot = reinterpret_cast<uint32_t*>(w + L.tot);
     const uint32_t passes = n ? (keys->bits + 7) / 8 : 0;
     const size_t scat_smem = (size_t)kGsTile * (4 + vbytes);
-    const size_t red_smem = (size_t)(kGsTile + 1) * (8 + 4);
+    const size_t red_smem = (size_t)(kGsTile + 1) * (8 + 4);  // run starts: running sum and position
     if (vbytes == 4) {
         e = cudaFuncSetAttribute(gs_scatter_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scat_smem);
         if (e == cudaSuccess)

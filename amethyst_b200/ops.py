@@ -207,9 +207,9 @@ def groupby_sort(keys: PackedColumn, vals: PackedColumn, key_fmt: int = A.PLAIN3
 def groupby_auto(keys: PackedColumn, vals: PackedColumn, groups_hint: int, **kw):
     """Group-by through the variant that the expected number of groups favours: the hash tables
     (amx_groupby) below n / 128 groups, radix sort + reduce-by-key (amx_groupby_sort) from there
-    on.  Measured on 2^26 32-bit keys (bench line groupby_wide): 100,000 groups 2.70 vs 4.78 ms
-    (hash faster), 2^20 groups 6.52 vs 4.91 ms, 2^23 groups 10.78 vs 5.11 ms, 6.7e7 groups 28.9 vs
-    6.05 ms (sort faster).  Keys of at most 24 bits always take the dense tables."""
+    on.  Measured on 2^26 32-bit keys (bench line groupby_wide): 100,000 groups 2.67 vs 3.19 ms
+    (hash faster), 2^20 groups 6.54 vs 3.30 ms, 2^23 groups 10.79 vs 3.51 ms, 6.7e7 groups 29.0 vs
+    5.30 ms (sort faster).  Keys of at most 24 bits always take the dense tables."""
     if keys.bits > 24 and groups_hint * 128 >= max(keys.n, 1):
         return groupby_sort(keys, vals, max_groups=kw.pop("max_groups", None) or max(1, min(keys.n, groups_hint * 2)),
                             **{k: v for k, v in kw.items() if k != "ws"})
