@@ -114,3 +114,26 @@ def test_groupby_sort_agrees_with_the_hash_group_by(cuda):
         for x, y in zip(a[:3], b[:3]):
             nb = O.storage_bytes(x.fmt, x.bits, g)
             assert torch.equal(x.data[:nb], y.data[:nb])
+
+
+def test_groupby_auto_picks_by_expected_groups(cuda):
+    """ops.groupby_auto: the hash tables below n / 128 expected groups, the sort from there on;
+    both give the oracle's groups."""
+    from unittest import mock
+
+    from amethyst_b200 import ops
+
+    n, kb = 100003, 32
+    keys = wide_keys(n, kb, 20000, 4)
+    kv, kraw = make_column(41, SLAB, kb, n, vals=keys)
+    vv, vraw = make_column(42, SLAB, 16, n)
+    kc, vc = to_gpu(kraw, n, SLAB, kb), to_gpu(vraw, n, SLAB, 16)
+    g, wk, ws, wc = O.groupby_sorted(kraw, SLAB, kb, vraw, SLAB, 16, n)
+    for hint, expect_sort in ((100, False), (n // 128 + 1, True), (20000, True)):
+        with mock.patch.object(ops, "groupby_sort", wraps=ops.groupby_sort) as gs:
+            ok, osum, ocnt, ng = ops.groupby_auto(kc, vc, hint, max_groups=1 << 16)
+        assert gs.called == expect_sort, hint
+        assert int(ng[0].item()) == g
+        assert np.array_equal(gpu_bytes(ok, g).view(np.uint32), wk.astype(np.uint32))
+        assert np.array_equal(gpu_bytes(osum, g).view(np.uint64), ws)
+        assert np.array_equal(gpu_bytes(ocnt, g).view(np.uint64), wc)
