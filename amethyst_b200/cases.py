@@ -9,6 +9,7 @@ larger than the 126 MB L2 unless the case says otherwise.
   chain      A 2^26 x u7 slabs + B 2^26 x u13 slabs -> C at 14 bits, keep C >= 2^13, compressstore
              to 14-bit slabs, sum (one amx_chain call)
   fcB        filter v < 205 * 2^(B-11) + compressstore over 2^24 slabs of width B (e.g. fc11)
+  fc_cfg1    filter v < 205 + compressstore over 2^24 elements in 11-bit slabs (26.8 MB)
   filterB    filter -> bitmask over 2^24 slabs of width B
   matmul     4096^3 u7 x u7 slab matrices -> narrowest-width slabs (unpack + GEMM + pack)
   matmul_fused  the same through the fused kernel (amx_tuning.policy 2)
@@ -75,8 +76,9 @@ def case(name: str, reps: int = 10) -> dict:
         return {"case": name, "ms": ms, "GB_s": byts / ms / 1e6}
     if name.startswith("fc") or name.startswith("filter"):
         flt = name.startswith("filter")
-        bits = int(name[6:] if flt else name[2:])
-        n = (1 << 24) * (64 // bits)
+        small = name == "fc_cfg1"  # the plain configuration: 2^24 elements (not slabs) at 11 bits
+        bits = 11 if small else int(name[6:] if flt else name[2:])
+        n = (1 << 24) if small else (1 << 24) * (64 // bits)
         col = _gen(n, bits, 0xC0FFEE)
         ws = ops.workspace(n)
         thr = (205 << (bits - 11)) if bits >= 11 else max(1, 205 >> (11 - bits))
