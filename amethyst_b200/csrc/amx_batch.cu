@@ -133,7 +133,44 @@ struct BatchPending {
     uint64_t eps_m64;
     uint32_t total, bits, eps, cv16, last, ci;
     unsigned long long sum;
+    uint64_t item, first;  // the item and its column's first item (for the deferred look-back)
 };
+
+// Decoupled look-back of item `item` (warp 0): the survivors of the column's items before it.
+// Every item publishes its own count (kBatchA) right after its block scan and its inclusive
+// prefix (kBatchP) once this look-back is done.
+__device__ __forceinline__ uint64_t batch_lookback(uint64_t* status, uint64_t item, uint64_t first, uint32_t total,
+                                                   BatchHdr* hdr, uint32_t lane)
+{
+    uint64_t excl = 0;
+    uint64_t jj = item;  // items [first, jj) remain to be visited
+    bool done = item == first;
+    while (!done) {
+        const bool in = jj > first + lane;
+        const uint64_t idx = jj - 1 - lane;
+        uint64_t st = in ? ld_relaxed_u64(&status[idx]) : kBatchP;
+        uint32_t spins = 0;
+        while (in && (st & (kBatchP | kBatchA)) == 0) {
+            if (++spins > kWaitSpins) {
+                record_error(&hdr->err, AMX_ERR_TIMEOUT);
+                st = kBatchP;
+                break;
+            }
+            if (spins > 8) __nanosleep(32);
+            st = ld_relaxed_u64(&status[idx]);
+        }
+        const uint32_t pmask = __ballot_sync(0xffffffffu, (st & kBatchP) != 0);
+        const uint32_t stop = pmask ? (uint32_t)(__ffs(pmask) - 1) : 31;
+        uint64_t v = (in && lane <= stop) ? (st & kBatchVal) : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        done = pmask != 0;
+        jj = jj > 32 ? jj - 32 : 0;
+    }
+    if (item != first && lane == 0) st_relaxed_u64(&status[item], kBatchP | (excl + total));
+    return excl;
+}
 
 template <uint32_t THREADS>
 __device__ __forceinline__ void batch_encode(const BatchPending& q, const uint8_t* cvbuf, uint32_t tid,
@@ -180,8 +217,15 @@ __global__ void __launch_bounds__(THREADS, THREADS == 512 ? 2 : 4) batch_fc_kern
     bool pending = false;
 
     for (;;) {
+        // the previous item's look-back, deferred to here: its prefix is only needed by its
+        // encode below, and by now its predecessors have mostly published theirs
+        if (pending && warp == 0) {
+            const uint64_t excl = batch_lookback(status, pend.item, pend.first, pend.total, hdr, lane);
+            if (lane == 0) s_excl = excl;
+        }
         if (tid == 0) s_item = atomicAdd(&hdr->ticket, 1ull);
-        __syncthreads();  // the ticket; also every read of the previous item's shared values is done
+        __syncthreads();  // the ticket and the previous item's prefix; every read of its shared values is done
+        if (pending) pend.g0 = s_excl;
         const uint64_t item = s_item;
         if (item >= total_items) break;
         const uint32_t ci = __ldg(colmap + item);
@@ -192,7 +236,6 @@ __global__ void __launch_bounds__(THREADS, THREADS == 512 ? 2 : 4) batch_fc_kern
         const uint32_t valid = rem < c.te ? (uint32_t)rem : c.te;
         const uint32_t R = c.spt * c.eps;
         const uint32_t B = c.bits;
-        const uint64_t FM = (1ull << B) - 1;
 
         // 1. this item's slab words, loads in flight ...
         uint64_t x[kBatchMaxSpt], g[kBatchMaxSpt];
@@ -234,45 +277,11 @@ __global__ void __launch_bounds__(THREADS, THREADS == 512 ? 2 : 4) batch_fc_kern
         }
         const uint32_t pos0 = before + incl - cnt;
 
-        // 5. decoupled look-back inside the column (warp 0) ...
-        if (warp == 0) {
-            uint64_t excl = 0;
-            if (t == 0) {
-                if (lane == 0) st_relaxed_u64(&status[item], kBatchP | total);
-            }
-            else {
-                if (lane == 0) st_relaxed_u64(&status[item], kBatchA | total);
-                uint64_t jj = item;  // items [c.item0, jj) remain to be visited
-                bool done = false;
-                while (!done) {
-                    const bool in = jj > c.item0 + lane;
-                    const uint64_t idx = jj - 1 - lane;
-                    uint64_t st = in ? ld_relaxed_u64(&status[idx]) : kBatchP;
-                    uint32_t spins = 0;
-                    while (in && (st & (kBatchP | kBatchA)) == 0) {
-                        if (++spins > kWaitSpins) {
-                            record_error(&hdr->err, AMX_ERR_TIMEOUT);
-                            st = kBatchP;
-                            break;
-                        }
-                        if (spins > 8) __nanosleep(32);
-                        st = ld_relaxed_u64(&status[idx]);
-                    }
-                    const uint32_t pmask = __ballot_sync(0xffffffffu, (st & kBatchP) != 0);
-                    const uint32_t stop = pmask ? (uint32_t)(__ffs(pmask) - 1) : 31;
-                    uint64_t v = (in && lane <= stop) ? (st & kBatchVal) : 0;
-#pragma unroll
-                    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    excl += v;
-                    done = pmask != 0;
-                    jj = jj > 32 ? jj - 32 : 0;
-                }
-                if (lane == 0) st_relaxed_u64(&status[item], kBatchP | (excl + total));
-            }
-            if (lane == 0) s_excl = excl;
-        }
+        // 5. this item's count for the look-backs of the column's later items (the first item's
+        // count is already its inclusive prefix); its own look-back waits for the next iteration
+        if (tid == 0) st_relaxed_u64(&status[item], (t == 0 ? kBatchP : kBatchA) | total);
 
-        // ... while every warp gathers its survivors and sums them
+        // every warp gathers its survivors and sums them
         unsigned long long mysum = 0;
         {
             const bool dense = 25 * __reduce_add_sync(0xffffffffu, cnt) > 32 * R;  // above ~4% survivors
@@ -287,11 +296,13 @@ __global__ void __launch_bounds__(THREADS, THREADS == 512 ? 2 : 4) batch_fc_kern
 #pragma unroll
         for (int o = 16; o; o >>= 1) mysum += __shfl_xor_sync(0xffffffffu, mysum, o);
         if (lane == 0) s_wsum[warp] = mysum;
-        __syncthreads();  // survivors gathered, s_excl and the warp sums visible
+        __syncthreads();  // survivors gathered, the warp sums visible
 
         // the encode waits for the next item's loads to be in flight (step 2)
         pend.out = c.out;
-        pend.g0 = s_excl;
+        pend.g0 = 0;  // set after the next look-back
+        pend.item = item;
+        pend.first = c.item0;
         pend.eps_m64 = c.eps_m64;
         pend.total = total;
         pend.bits = B;
@@ -304,7 +315,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == 512 ? 2 : 4) batch_fc_kern
             for (uint32_t w = 0; w < NW; w++) pend.sum += s_wsum[w];
         pending = true;
     }
-    if (pending) batch_encode<THREADS>(pend, cvbuf, tid, counts, sums);
+    if (pending) batch_encode<THREADS>(pend, cvbuf, tid, counts, sums);  // its prefix came with the last ticket
 }
 
 }  // namespace amx
