@@ -78,7 +78,7 @@ __host__ __device__ constexpr uint64_t swar_top_bits(int b)
 // aggregate, no bitmask), so the kernel carries only that path: less code for the instruction
 // cache to hold next to the other warp roles.  FILTER: likewise for a request that only writes
 // the bitmask; AGGONLY: for one that only counts and aggregates.
-template <int B, bool PLAIN = false, bool FILTER = false, bool AGGONLY = false>
+template <int B, bool PLAIN = false, bool FILTER = false, bool AGGONLY = false, bool NARROW = false>
 struct SwarPol {
     using V = uint32_t;
     static constexpr int kBits = B;
@@ -93,7 +93,9 @@ struct SwarPol {
     static constexpr bool kMap = false;
     // the plain compressstore at widths of at most 5 fields per slab runs 24 compute warps (its
     // registers allow 960 threads): more warps to hide the compute warps' latencies
-    static constexpr uint32_t kCompute = ((PLAIN || FILTER || AGGONLY) && EPS * SPT <= 40) ? 768 : 512;
+    // (NARROW: 16 compute warps always -- the plain compressstore by an input mask, whose mask
+    // stage would leave the 24-warp form one survivor slot)
+    static constexpr uint32_t kCompute = ((PLAIN || FILTER || AGGONLY) && EPS * SPT <= 40 && !NARROW) ? 768 : 512;
     static constexpr int kMinBlocks = 1;
     static constexpr uint64_t kField = (1ull << B) - 1;  // one field
     static constexpr uint64_t kTop = swar_top_bits(B);    // the top bit of every field

@@ -12,12 +12,13 @@ amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t 
         return launch<SwarPol<B, false, false, true>>(p, ws, ws_bytes, stream);
     if constexpr (B <= 16) {
         // the plain compressstore takes the kernel that carries only its own path; with an input
-        // mask only in its 16-warp form: the 24-warp form's two stages and two survivor slots
-        // fill the 227 KB, and the mask's stage would leave room for one slot (compute warps then
-        // wait for the encoder every tile: 0.25 vs 0.11 ms on a one-cluster mask)
+        // mask in its 16-warp form: the 24-warp form's two stages and two survivor slots fill the
+        // 227 KB, and the mask's stage would leave room for one slot (compute warps then wait for
+        // the encoder every tile: 0.25 vs 0.11 ms on a one-cluster mask)
         if (p.has_out && p.compact && !p.has_agg && !p.mask_out && p.out.format == AMX_SLAB && p.out.bits == B &&
-            p.vbits <= 16 && (!p.has_mask_in || SwarPol<B, true>::kCompute == 512))
-            return launch<SwarPol<B, true>>(p, ws, ws_bytes, stream);
+            p.vbits <= 16)
+            return p.has_mask_in ? launch<SwarPol<B, true, false, false, true>>(p, ws, ws_bytes, stream)
+                                 : launch<SwarPol<B, true>>(p, ws, ws_bytes, stream);
     }
     return launch<SwarPol<B>>(p, ws, ws_bytes, stream);
 }
