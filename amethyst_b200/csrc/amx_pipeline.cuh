@@ -683,10 +683,19 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             }
             else if constexpr (Pol::kAggOnly) {
                 if (p.has_agg) {
-                    const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
-                    uint64_t a = 0;
-                    swar_visit<B, SPT, uint32_t, false, true>(x, g, 25 * wc > 32 * (uint32_t)R, nullptr, 0, p.agg, a);
-                    my_agg = agg_combine(p.agg, my_agg, a);
+                    bool done = false;
+                    if constexpr (swar_sum_fits<B, SPT>()) {
+                        if (p.agg == AMX_AGG_SUM) {  // field-parallel: no field extracted
+                            my_agg += swar_masked_sum<B, SPT>(x, g);
+                            done = true;
+                        }
+                    }
+                    if (!done) {
+                        const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
+                        uint64_t a = 0;
+                        swar_visit<B, SPT, uint32_t, false, true>(x, g, 25 * wc > 32 * (uint32_t)R, nullptr, 0, p.agg, a);
+                        my_agg = agg_combine(p.agg, my_agg, a);
+                    }
                 }
             }
             else if constexpr (Pol::kPlain) {

@@ -207,6 +207,54 @@ __device__ __forceinline__ void swar_flags(uint32_t mode, const uint64_t (&x)[N]
     }
 }
 
+// Sum of the passing fields of a thread's SPT words, field-parallel: the flags (top bits of the
+// passing fields) times the field mask give whole-field masks (each product term fills exactly its
+// own field: no carries), and the even and the odd fields accumulate in two words whose lanes are
+// two fields wide.  swar_sum_fits<B, SPT>() says whether every lane holds the sum of SPT fields
+// (tests/test_swar_cpu.py models it against field-by-field sums); the others sum field by field.
+template <int B, int SPT>
+__host__ __device__ constexpr bool swar_sum_fits()
+{
+    int need = B;
+    for (int s = SPT; s > 0; s >>= 1) need++;  // B + bit length of SPT
+    for (int k = 0; k < 64 / B; k++) {
+        int room = (k % 2 == 0) ? 64 - k * B : 64 - B - (k - 1) * B;  // odd fields are shifted down by B
+        if (room > 2 * B) room = 2 * B;
+        if (room < need) return false;
+    }
+    return true;
+}
+
+template <int B, int SPT>
+__device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], const uint64_t (&g)[SPT])
+{
+    constexpr int EPS = 64 / B;
+    constexpr uint64_t FM = (1ull << B) - 1;
+    constexpr uint64_t EVEN = [] {
+        uint64_t e = 0;
+        for (int k = 0; k < 64 / B; k += 2) e |= ((1ull << B) - 1) << (k * B);
+        return e;
+    }();
+    uint64_t a = 0, b = 0;
+#pragma unroll
+    for (int i = 0; i < SPT; i++) {
+        const uint64_t m = x[i] & ((g[i] >> (B - 1)) * FM);
+        a += m & EVEN;
+        b += (m >> B) & EVEN;
+    }
+    uint64_t t = 0;
+#pragma unroll
+    for (int k = 0; k < EPS; k += 2) {
+        const int ra = 64 - k * B < 2 * B ? 64 - k * B : 2 * B;
+        t += (a >> (k * B)) & (ra >= 64 ? ~0ull : ((1ull << ra) - 1));
+        if (k + 1 < EPS) {
+            const int rb = 64 - B - k * B < 2 * B ? 64 - B - k * B : 2 * B;
+            t += (b >> (k * B)) & (rb >= 64 ? ~0ull : ((1ull << rb) - 1));
+        }
+    }
+    return t;
+}
+
 // Visit the passing elements of a thread's run in element order: store each value to dst[pos++]
 // (when DST) and fold it into the aggregate `a` (when AGG).  Dense warps walk every field with a
 // predicated store (no branches, independent extractions); sparse warps walk the set flag bits

@@ -75,3 +75,50 @@ def test_flag_deposit_places_every_pattern():
         if e < 64:
             noisy = pats | (rng.integers(0, 1 << 63, size=pats.size, dtype=np.uint64) << np.uint64(e))
             assert np.array_equal(deposit(b, noisy), want), b
+
+
+def sum_fits(b, spt):
+    """swar_sum_fits<B, SPT>(): every two-field lane holds the sum of SPT fields."""
+    need = b + spt.bit_length()
+    for k in range(64 // b):
+        room = 64 - k * b if k % 2 == 0 else 64 - b - (k - 1) * b
+        if min(room, 2 * b) < need:
+            return False
+    return True
+
+
+def test_field_parallel_masked_sum():
+    """swar_masked_sum: whole-field masks from the flags by one product, even and odd fields summed
+    in two-field lanes, against field-by-field sums of the passing fields (random words with junk
+    padding bits, every flag pattern style), for every width whose lanes hold SPT sums."""
+    rng = np.random.default_rng(3)
+    fits = []
+    for b in range(1, 33):
+        e = 64 // b
+        spt = 1 if e >= 64 else min(8, 64 // e)
+        if not sum_fits(b, spt):
+            continue
+        fits.append(b)
+        fm = (1 << b) - 1
+        top = sum(1 << (k * b + b - 1) for k in range(e))
+        even = sum(fm << (k * b) for k in range(0, e, 2))
+        for trial in range(400):
+            words = [int(w) for w in rng.integers(0, 1 << 63, size=spt, dtype=np.uint64) * 2 + 1]
+            if trial % 3 == 0:  # every field at its maximum, junk above the fields
+                words = [sum(fm << (k * b) for k in range(e)) | (w & ~((1 << (e * b)) - 1) & M64) for w in words]
+            flags = [int(f) & top for f in rng.integers(0, 1 << 63, size=spt, dtype=np.uint64) * 2]
+            if trial % 5 == 0:
+                flags = [top] * spt
+            a = bb = 0
+            for x, g in zip(words, flags):
+                m = x & (((g >> (b - 1)) * fm) & M64)
+                a = (a + (m & even)) & M64
+                bb = (bb + ((m >> b) & even)) & M64
+            got = 0
+            for k in range(0, e, 2):
+                got += (a >> (k * b)) & ((1 << min(64 - k * b, 2 * b)) - 1)
+                if k + 1 < e:
+                    got += (bb >> (k * b)) & ((1 << min(64 - b - k * b, 2 * b)) - 1)
+            want = sum((x >> (k * b)) & fm for x, g in zip(words, flags) for k in range(e) if (g >> (k * b + b - 1)) & 1)
+            assert got == want, (b, trial)
+    assert fits == [5, 6, 10, 11, 12, 13, 14, 15, 17, 18, 19, 20, 22, 23, 24, 25, 26, 27, 28, 29, 30]
