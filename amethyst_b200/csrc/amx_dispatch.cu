@@ -97,7 +97,7 @@ amx_status run_chain(const ChainReq& r, void* ws, size_t ws_bytes, cudaStream_t 
         if (p.has_pred) {
             swar_setup(p);
         }
-        else {  // an input mask alone: every field passes the (absent) predicate
+        else {  // an input mask or an aggregate alone: every field passes the (absent) predicate
             p.sw_mode = 0;
             p.sw_l1 = p.sw_l2 = 0;
         }

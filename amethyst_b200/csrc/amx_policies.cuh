@@ -251,10 +251,15 @@ constexpr int kSwarPolicyBase = 200;
 #define AMX_PAIR(a, b) Slab2Pol<a, b>
 
 // A request the field-parallel slab policy (SwarPol) serves: one slab column of width <= 32, a
-// predicate on the field values themselves and/or an input mask, and a compacted output or none.
+// predicate on the field values themselves and/or an input mask, and a compacted output or none;
+// or a sum alone at a width whose field-parallel sum fits (every field passes; 1 GiB-class column
+// at 11 bits 0.234 vs 0.366 ms with the compile-time policy, while at 16 bits, summed field by
+// field, it measured slower: 0.381 vs 0.334 ms).
 inline bool swar_applicable(const PipeParams& p)
 {
-    return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && (p.has_pred || p.has_mask_in) &&
+    const bool agg_alone = !p.has_out && !p.mask_out && p.has_agg && p.agg == AMX_AGG_SUM && p.a.bits <= 32 &&
+                           swar_sum_fits_slab((int)p.a.bits);
+    return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && (p.has_pred || p.has_mask_in || agg_alone) &&
            (!p.has_out || p.compact) && p.op == AMX_OP_LHS && !p.need_vmask && p.vbits <= 32;
 }
 

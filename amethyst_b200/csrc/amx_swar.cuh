@@ -212,8 +212,7 @@ __device__ __forceinline__ void swar_flags(uint32_t mode, const uint64_t (&x)[N]
 // own field: no carries), and the even and the odd fields accumulate in two words whose lanes are
 // two fields wide.  swar_sum_fits<B, SPT>() says whether every lane holds the sum of SPT fields
 // (tests/test_swar_cpu.py models it against field-by-field sums); the others sum field by field.
-template <int B, int SPT>
-__host__ __device__ constexpr bool swar_sum_fits()
+__host__ __device__ constexpr bool swar_sum_fits_w(int B, int SPT)
 {
     int need = B;
     for (int s = SPT; s > 0; s >>= 1) need++;  // B + bit length of SPT
@@ -224,6 +223,23 @@ __host__ __device__ constexpr bool swar_sum_fits()
     }
     return true;
 }
+
+template <int B, int SPT>
+__host__ __device__ constexpr bool swar_sum_fits()
+{
+    return swar_sum_fits_w(B, SPT);
+}
+
+// The same for SwarPol<B>'s own SPT (min(8, 64 / EPS), 1 at EPS = 64), at a width known at run time
+__host__ __device__ constexpr bool swar_sum_fits_slab(int B)
+{
+    return swar_sum_fits_w(B, 64 / B >= 64 ? 1 : (64 / (64 / B) < 8 ? 64 / (64 / B) : 8));
+}
+static_assert(swar_sum_fits_slab(7) == swar_sum_fits<7, SwarPol<7>::SPT>() &&
+                  swar_sum_fits_slab(11) == swar_sum_fits<11, SwarPol<11>::SPT>() &&
+                  swar_sum_fits_slab(16) == swar_sum_fits<16, SwarPol<16>::SPT>() &&
+                  swar_sum_fits_slab(1) == swar_sum_fits<1, SwarPol<1>::SPT>(),
+              "host rule follows the policy's SPT");
 
 template <int B, int SPT>
 __device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], const uint64_t (&g)[SPT])
