@@ -690,6 +690,12 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                             done = true;
                         }
                     }
+                    else if constexpr (B <= kSwarPlaneMax) {
+                        if (p.agg == AMX_AGG_SUM) {
+                            my_agg += swar_plane_sum<B, SPT>(x, g);
+                            done = true;
+                        }
+                    }
                     if (!done) {
                         const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
                         uint64_t a = 0;

@@ -252,13 +252,15 @@ constexpr int kSwarPolicyBase = 200;
 
 // A request the field-parallel slab policy (SwarPol) serves: one slab column of width <= 32, a
 // predicate on the field values themselves and/or an input mask, and a compacted output or none;
-// or a sum alone at a width whose field-parallel sum fits (every field passes; 1 GiB-class column
-// at 11 bits 0.234 vs 0.366 ms with the compile-time policy, while at 16 bits, summed field by
-// field, it measured slower: 0.381 vs 0.334 ms).
+// or a sum alone (every field passes) at a width whose field-parallel or bit-plane sum applies, or
+// at 7 bits (field visit).  1 GiB-class column against the compile-time policy: 11 bits 0.234 vs
+// 0.366 ms, 3 bits 0.157 vs 0.479, 7 bits 0.263 vs 0.397; at 16 bits, summed field by field, it
+// measured slower (0.381 vs 0.334 ms), at 8 and 9 bits by bit planes too.
 inline bool swar_applicable(const PipeParams& p)
 {
-    const bool agg_alone = !p.has_out && !p.mask_out && p.has_agg && p.agg == AMX_AGG_SUM && p.a.bits <= 32 &&
-                           swar_sum_fits_slab((int)p.a.bits);
+    const int b = (int)p.a.bits;
+    const bool agg_alone = !p.has_out && !p.mask_out && p.has_agg && p.agg == AMX_AGG_SUM && b <= 32 &&
+                           (swar_sum_fits_slab(b) || b <= kSwarPlaneMax || b == 7);
     return !p.has_b && p.a.format == AMX_SLAB && p.a.bits <= 32 && (p.has_pred || p.has_mask_in || agg_alone) &&
            (!p.has_out || p.compact) && p.op == AMX_OP_LHS && !p.need_vmask && p.vbits <= 32;
 }

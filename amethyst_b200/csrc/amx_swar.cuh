@@ -271,6 +271,37 @@ __device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], co
     return t;
 }
 
+// Sum of the passing fields by bit planes, for the narrow widths whose lanes swar_masked_sum cannot
+// hold: the passing fields (whole-field masks as there) are counted per bit position b and each
+// count weighted by 2^b.  B population counts per word, nothing to overflow.  Up to 4 bits (1 GiB-
+// class column, 671M fields, no predicate: 3 bits 0.157 vs 0.479 ms with the compile-time policy);
+// at 7 bits the field visit is faster (0.263 vs 0.312 ms), at 8 and 9 the compile-time policy.
+constexpr int kSwarPlaneMax = 4;
+
+template <int B, int SPT>
+__device__ __forceinline__ uint64_t swar_plane_sum(const uint64_t (&x)[SPT], const uint64_t (&g)[SPT])
+{
+    constexpr uint64_t FM = (1ull << B) - 1;
+    constexpr uint64_t LOW = [] {
+        uint64_t e = 0;
+        for (int k = 0; k < 64 / B; k++) e |= 1ull << (k * B);
+        return e;
+    }();
+    uint32_t cnt[B];
+#pragma unroll
+    for (int b = 0; b < B; b++) cnt[b] = 0;
+#pragma unroll
+    for (int i = 0; i < SPT; i++) {
+        const uint64_t m = x[i] & ((g[i] >> (B - 1)) * FM);
+#pragma unroll
+        for (int b = 0; b < B; b++) cnt[b] += __popcll(m & (LOW << b));
+    }
+    uint64_t t = 0;
+#pragma unroll
+    for (int b = 0; b < B; b++) t += (uint64_t)cnt[b] << b;
+    return t;
+}
+
 // Visit the passing elements of a thread's run in element order: store each value to dst[pos++]
 // (when DST) and fold it into the aggregate `a` (when AGG).  Dense warps walk every field with a
 // predicated store (no branches, independent extractions); sparse warps walk the set flag bits

@@ -177,3 +177,24 @@ def test_swar_mask_input(cuda, restore_tuning, bits):
             for agg in (A.AGG_SUM, A.AGG_MAX, A.AGG_XOR):
                 got = int(ops.reduce(agg, col, dm).cpu().numpy().view(np.uint64)[0])
                 assert got == O.reduce(agg, raw, n, SLAB, bits, m), (bits, mi, agg)
+
+
+@pytest.mark.parametrize("bits", list(range(1, 33)))
+def test_sum_alone_every_width(cuda, restore_tuning, bits):
+    """A sum with neither predicate nor mask (field-parallel lanes, bit planes up to 4 bits, a field
+    visit or the compile-time policy, by width): random columns and columns of maximal fields,
+    ragged tails, against the oracle bit-exact; forced and automatic policy choice agree."""
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    top = (1 << bits) - 1
+    for n in (1, 4097, 300001):
+        _, raw = make_column(bits * 17 + n, SLAB, bits, n)
+        full = O.encode(SLAB, bits, np.full(n, top, np.uint64))
+        for r in (raw, full):
+            col = to_gpu(r, n, SLAB, bits)
+            want = O.reduce(A.AGG_SUM, r, n, SLAB, bits)
+            for force in (0, 1 + SWAR_BASE + bits):
+                _set_policy(force)
+                got = int(ops.hop(A.AGG_SUM, col).cpu().numpy().view(np.uint64)[0])
+                assert got == want, (bits, n, force)

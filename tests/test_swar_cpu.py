@@ -122,3 +122,30 @@ def test_field_parallel_masked_sum():
             want = sum((x >> (k * b)) & fm for x, g in zip(words, flags) for k in range(e) if (g >> (k * b + b - 1)) & 1)
             assert got == want, (b, trial)
     assert fits == [5, 6, 10, 11, 12, 13, 14, 15, 17, 18, 19, 20, 22, 23, 24, 25, 26, 27, 28, 29, 30]
+
+
+def test_bit_plane_sum():
+    """swar_plane_sum: the passing fields' bits counted per bit position b and weighted by 2^b,
+    against field-by-field sums, for the narrow widths, up to 9 bits (the kernel takes it up to 4)."""
+    rng = np.random.default_rng(4)
+    for b in range(1, 10):
+        e = 64 // b
+        spt = 1 if e >= 64 else min(8, 64 // e)
+        fm = (1 << b) - 1
+        top = sum(1 << (k * b + b - 1) for k in range(e))
+        low = sum(1 << (k * b) for k in range(e))
+        for trial in range(300):
+            words = [int(w) for w in rng.integers(0, 1 << 63, size=spt, dtype=np.uint64) * 2 + 1]
+            if trial % 3 == 0:
+                words = [sum(fm << (k * b) for k in range(e)) | (w & ~((1 << (e * b)) - 1) & M64) for w in words]
+            flags = [int(f) & top for f in rng.integers(0, 1 << 63, size=spt, dtype=np.uint64) * 2]
+            if trial % 5 == 0:
+                flags = [top] * spt
+            cnt = [0] * b
+            for x, g in zip(words, flags):
+                m = x & (((g >> (b - 1)) * fm) & M64)
+                for p in range(b):
+                    cnt[p] += bin(m & ((low << p) & M64)).count("1")
+            got = sum(c << p for p, c in enumerate(cnt))
+            want = sum((x >> (k * b)) & fm for x, g in zip(words, flags) for k in range(e) if (g >> (k * b + b - 1)) & 1)
+            assert got == want, (b, trial)
