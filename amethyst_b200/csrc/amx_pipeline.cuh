@@ -706,9 +706,13 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             }
             else if constexpr (Pol::kPlain) {
                 const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
-                uint64_t a = 0;
-                swar_visit<B, SPT, uint16_t, true, false>(x, g, 25 * wc > 32 * (uint32_t)R,
-                                                          reinterpret_cast<uint16_t*>(slot), pos, 0, a);
+                if (25 * wc > 32 * (uint32_t)R) {
+                    swar_store_dense_raw<B, SPT>(x, g, reinterpret_cast<uint16_t*>(slot) + pos);
+                }
+                else {
+                    uint64_t a = 0;
+                    swar_visit<B, SPT, uint16_t, true, false>(x, g, false, reinterpret_cast<uint16_t*>(slot), pos, 0, a);
+                }
             }
             else if (p.has_out || p.has_agg) {
                 // the walk over set bits wins only below ~4% survivors in the warp

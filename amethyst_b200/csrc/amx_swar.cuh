@@ -302,6 +302,36 @@ __device__ __forceinline__ uint64_t swar_plane_sum(const uint64_t (&x)[SPT], con
     return t;
 }
 
+// Dense walk of the plain compressstore: for every field whose flag is set, the low 16 bits from
+// the field's first bit on (the field, then bits of the next one, which the slab encoder masks off)
+// stored at the running position.  Works on the 32-bit halves of each word: a field costs a flag
+// test, one shift (none for field 0; a funnel shift for the field across the halves), and the
+// predicated store and advance.
+template <int B, int SPT>
+__device__ __forceinline__ void swar_store_dense_raw(const uint64_t (&x)[SPT], const uint64_t (&g)[SPT],
+                                                     uint16_t* d)
+{
+    constexpr int EPS = 64 / B;
+#pragma unroll
+    for (int i = 0; i < SPT; i++) {
+        const uint32_t lo = (uint32_t)x[i], hi = (uint32_t)(x[i] >> 32);
+        const uint32_t glo = (uint32_t)g[i], ghi = (uint32_t)(g[i] >> 32);
+#pragma unroll
+        for (int k = 0; k < EPS; k++) {
+            const int sb = k * B, fb = sb + B - 1;
+            const bool pass = fb < 32 ? ((glo >> fb) & 1u) != 0 : ((ghi >> (fb - 32)) & 1u) != 0;
+            uint32_t v;
+            if (sb >= 32)
+                v = hi >> (sb - 32);
+            else if (sb + B <= 32)
+                v = lo >> sb;
+            else
+                v = __funnelshift_r(lo, hi, sb);
+            if (pass) *d++ = (uint16_t)v;
+        }
+    }
+}
+
 // Visit the passing elements of a thread's run in element order: store each value to dst[pos++]
 // (when DST) and fold it into the aggregate `a` (when AGG).  Dense warps walk every field with a
 // predicated store (no branches, independent extractions); sparse warps walk the set flag bits
