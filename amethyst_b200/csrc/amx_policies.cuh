@@ -254,8 +254,8 @@ constexpr int kSwarPolicyBase = 200;
 // predicate on the field values themselves and/or an input mask, and a compacted output or none;
 // or a sum alone (every field passes) at a width whose field-parallel or bit-plane sum applies, or
 // at 7 bits (field visit).  1 GiB-class column against the compile-time policy: 11 bits 0.234 vs
-// 0.366 ms, 3 bits 0.157 vs 0.479, 7 bits 0.263 vs 0.397; at 16 bits, summed field by field, it
-// measured slower (0.381 vs 0.334 ms), at 8 and 9 bits by bit planes too.
+// 0.366 ms, 8 bits 0.178 vs 0.336, 32 bits 0.473 vs 0.763, 3 bits 0.157 vs 0.479, 7 bits 0.263 vs
+// 0.397; at 9 and 21 bits, summed field by field, it measured slower (9 bits 0.482 vs 0.375 ms).
 inline bool swar_applicable(const PipeParams& p)
 {
     const int b = (int)p.a.bits;

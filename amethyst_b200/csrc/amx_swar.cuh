@@ -217,7 +217,9 @@ __host__ __device__ constexpr bool swar_sum_fits_w(int B, int SPT)
     int need = B;
     for (int s = SPT; s > 0; s >>= 1) need++;  // B + bit length of SPT
     for (int k = 0; k < 64 / B; k++) {
-        int room = (k % 2 == 0) ? 64 - k * B : 64 - B - (k - 1) * B;  // odd fields are shifted down by B
+        // odd fields are shifted down by B: odd field k's lane starts at bit (k - 1) B, and the top
+        // lane of either accumulator may grow to bit 63
+        int room = (k % 2 == 0) ? 64 - k * B : 64 - (k - 1) * B;
         if (room > 2 * B) room = 2 * B;
         if (room < need) return false;
     }
@@ -264,7 +266,7 @@ __device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], co
         const int ra = 64 - k * B < 2 * B ? 64 - k * B : 2 * B;
         t += (a >> (k * B)) & (ra >= 64 ? ~0ull : ((1ull << ra) - 1));
         if (k + 1 < EPS) {
-            const int rb = 64 - B - k * B < 2 * B ? 64 - B - k * B : 2 * B;
+            const int rb = ra;  // odd field k + 1, shifted down to bit k B
             t += (b >> (k * B)) & (rb >= 64 ? ~0ull : ((1ull << rb) - 1));
         }
     }
@@ -275,7 +277,7 @@ __device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], co
 // hold: the passing fields (whole-field masks as there) are counted per bit position b and each
 // count weighted by 2^b.  B population counts per word, nothing to overflow.  Up to 4 bits (1 GiB-
 // class column, 671M fields, no predicate: 3 bits 0.157 vs 0.479 ms with the compile-time policy);
-// at 7 bits the field visit is faster (0.263 vs 0.312 ms), at 8 and 9 the compile-time policy.
+// at 7 bits the field visit is faster (0.263 vs 0.312 ms), at 9 the compile-time policy.
 constexpr int kSwarPlaneMax = 4;
 
 template <int B, int SPT>

@@ -81,7 +81,7 @@ def sum_fits(b, spt):
     """swar_sum_fits<B, SPT>(): every two-field lane holds the sum of SPT fields."""
     need = b + spt.bit_length()
     for k in range(64 // b):
-        room = 64 - k * b if k % 2 == 0 else 64 - b - (k - 1) * b
+        room = 64 - k * b if k % 2 == 0 else 64 - (k - 1) * b
         if min(room, 2 * b) < need:
             return False
     return True
@@ -118,10 +118,11 @@ def test_field_parallel_masked_sum():
             for k in range(0, e, 2):
                 got += (a >> (k * b)) & ((1 << min(64 - k * b, 2 * b)) - 1)
                 if k + 1 < e:
-                    got += (bb >> (k * b)) & ((1 << min(64 - b - k * b, 2 * b)) - 1)
+                    got += (bb >> (k * b)) & ((1 << min(64 - k * b, 2 * b)) - 1)
             want = sum((x >> (k * b)) & fm for x, g in zip(words, flags) for k in range(e) if (g >> (k * b + b - 1)) & 1)
             assert got == want, (b, trial)
-    assert fits == [5, 6, 10, 11, 12, 13, 14, 15, 17, 18, 19, 20, 22, 23, 24, 25, 26, 27, 28, 29, 30]
+    assert fits == [1, 2, 4, 5, 6, 8, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 22, 23, 24, 25, 26, 27, 28, 29, 30,
+                    31, 32]
 
 
 def test_bit_plane_sum():
