@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
     constexpr uint32_t T = Pol::kCompute;
     constexpr uint32_t NW = T / 32;
     constexpr uint32_t TILE = T * R;
-    static_assert(TILE / 32 * 4 <= kCvOff - kBitmapOff, "bitmap region");
+    static_assert(Pol::kWide || TILE / 32 * 4 <= kCvOff - kBitmapOff, "bitmap region");  // wide: no bitmap
     static_assert(NW <= 32, "warp arrays hold 32 compute warps");
     static_assert(!WM || R <= 32, "warp-major runs keep one ballot per lane");
     auto compute_bar = []() { compute_bar_n<T>(); };
@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
         run_len[0] = len;
         run_len[1] = (len + TILE - 1) / TILE;
     }
-    if (!WM)
+    if (!WM && !Pol::kWide)
         for (uint32_t i = tid; i < TILE / 32; i += blockDim.x) bitmap[i] = 0;
     __syncthreads();  // the last CTA-wide barrier: roles split below
     const uint64_t n = run_len[0], num_tiles = run_len[1];
@@ -616,16 +616,19 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     lds_words<SPT>(src, x);
                 // tiles of T*R elements, T a multiple of 256: a tile's mask starts on a 32-byte
                 // boundary, the first staged byte
-                if (p.has_mask_in) mb = bits_at_v<R>(reinterpret_cast<const uint32_t*>(st + p.m_off), tid * R);
+                if constexpr (!Pol::kWide)
+                    if (p.has_mask_in) mb = bits_at_v<R>(reinterpret_cast<const uint32_t*>(st + p.m_off), tid * R);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);  // the words are in registers: stage s is free
 
             uint64_t g[SPT];
             swar_flags<B, SPT>(p.sw_mode, x, g, p.sw_l1, p.sw_l2);
-            if (p.has_mask_in) {
+            if constexpr (!Pol::kWide) {
+                if (p.has_mask_in) {
 #pragma unroll
-                for (int i = 0; i < SPT; i++) g[i] &= swar_deposit_flags<B>(mb >> (i * EPS));
+                    for (int i = 0; i < SPT; i++) g[i] &= swar_deposit_flags<B>(mb >> (i * EPS));
+                }
             }
             const uint32_t le0 = tid * R;
             if (le0 + R > valid) {  // elements past the column's end do not pass
@@ -640,7 +643,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             for (int i = 0; i < SPT; i++) c += __popcll(g[i]);
             my_count += c;
 
-            if (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out)) {
+            if constexpr (!Pol::kWide) if (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out)) {
                 uint64_t fl = 0;
                 if constexpr (B >= 8) {  // one multiplication per word (swar_gather_flags)
 #pragma unroll
@@ -696,11 +699,14 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                             done = true;
                         }
                     }
-                    if (!done) {
-                        const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
-                        uint64_t a = 0;
-                        swar_visit<B, SPT, uint32_t, false, true>(x, g, 25 * wc > 32 * (uint32_t)R, nullptr, 0, p.agg, a);
-                        my_agg = agg_combine(p.agg, my_agg, a);
+                    if constexpr (!Pol::kWide) {
+                        if (!done) {
+                            const uint32_t wc = __reduce_add_sync(0xffffffffu, c);
+                            uint64_t a = 0;
+                            swar_visit<B, SPT, uint32_t, false, true>(x, g, 25 * wc > 32 * (uint32_t)R, nullptr, 0,
+                                                                      p.agg, a);
+                            my_agg = agg_combine(p.agg, my_agg, a);
+                        }
                     }
                 }
             }
@@ -746,7 +752,7 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
                     qphase ^= 1;
                 }
             }
-            if (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out)) {
+            if (!Pol::kWide && (Pol::kFilter || (!Pol::kPlain && !Pol::kAggOnly && p.mask_out))) {
                 compute_bar();
                 const uint32_t words = (valid + 31) / 32;
                 for (uint32_t i = tid; i < words; i += T) {
@@ -1129,6 +1135,7 @@ struct GenericPolT {
     static constexpr bool kFilter = false;
     static constexpr bool kAggOnly = false;
     static constexpr bool kMap = MAP;
+    static constexpr bool kWide = false;
     static constexpr int kOutBits = 0;         // the encoder warps use the runtime encoder
     static constexpr uint32_t kCompute = 512;  // one CTA of 16 compute warps per SM
     static constexpr int kMinBlocks = 1;

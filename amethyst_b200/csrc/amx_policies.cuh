@@ -83,6 +83,7 @@ struct SlabPol {
     static constexpr bool kFilter = false;
     static constexpr bool kAggOnly = false;
     static constexpr bool kMap = false;
+    static constexpr bool kWide = false;
     // one CTA per SM: 16 compute warps, or 8 for the register-heavy 64-element runs and for
     // widths >= 17 (10+ slabs per thread: a 16-warp tile would not fit twice in shared memory)
     static constexpr uint32_t kCompute = (R > 40 || B >= 17) ? 256 : 512;
@@ -166,6 +167,7 @@ struct Slab2Pol {
     static constexpr bool kFilter = false;
     static constexpr bool kAggOnly = false;
     static constexpr bool kMap = false;
+    static constexpr bool kWide = false;
     // output width the encoder warps pack at compile time (slabs of the op's natural width)
     static constexpr int kOutBits = OP >= 0 ? op_out_bits(OP, BA, BB) : 0;
     // the plain variants run 20 compute warps where two stages and two slots of 16-bit values

@@ -77,19 +77,23 @@ __host__ __device__ constexpr uint64_t swar_top_bits(int b)
 // known to be the plain compressstore (slabs of width B <= 16 out, 16-bit gathered values, no
 // aggregate, no bitmask), so the kernel carries only that path: less code for the instruction
 // cache to hold next to the other warp roles.  FILTER: likewise for a request that only writes
-// the bitmask; AGGONLY: for one that only counts and aggregates.
-template <int B, bool PLAIN = false, bool FILTER = false, bool AGGONLY = false, bool NARROW = false>
+// the bitmask; AGGONLY: for one that only counts and aggregates.  WIDE (with AGGONLY, for a count
+// and at most a sum, no input mask): 8 slabs per thread at every width, runs past 64 elements, as
+// no flag or mask word of the run is kept (1-4-bit columns: tiles of 4-12 KB otherwise).
+template <int B, bool PLAIN = false, bool FILTER = false, bool AGGONLY = false, bool NARROW = false,
+          bool WIDE = false>
 struct SwarPol {
     using V = uint32_t;
     static constexpr int kBits = B;
     static constexpr int EPS = 64 / B;
-    static constexpr int SPT = EPS >= 64 ? 1 : (64 / EPS < 8 ? 64 / EPS : 8);
+    static constexpr int SPT = WIDE ? 8 : (EPS >= 64 ? 1 : (64 / EPS < 8 ? 64 / EPS : 8));
     static constexpr int R = EPS * SPT;
     static constexpr bool kWarpMajor = false;
     static constexpr bool kSwar = true;
     static constexpr bool kPlain = PLAIN;
     static constexpr bool kFilter = FILTER;    // the request only writes the bitmask
     static constexpr bool kAggOnly = AGGONLY;  // the request only counts and aggregates
+    static constexpr bool kWide = WIDE;        // ... and at most sums, with no input mask
     static constexpr bool kMap = false;
     // the plain compressstore at widths of at most 5 fields per slab runs 24 compute warps (its
     // registers allow 960 threads): more warps to hide the compute warps' latencies
@@ -99,7 +103,7 @@ struct SwarPol {
     static constexpr int kMinBlocks = 1;
     static constexpr uint64_t kField = (1ull << B) - 1;  // one field
     static constexpr uint64_t kTop = swar_top_bits(B);    // the top bit of every field
-    static_assert(R <= 64, "a thread's run must fit one 64-bit flag word");
+    static_assert(R <= 64 || (WIDE && AGGONLY), "a thread's run must fit one 64-bit flag word");
     static_assert(!PLAIN || B <= 16, "the plain compressstore gathers 16-bit values");
 };
 

@@ -8,8 +8,13 @@ amx_status launch_swar_w(PipeParams& p, void* ws, size_t ws_bytes, cudaStream_t 
 {
     if (!p.has_out && !p.has_agg && p.mask_out)  // the filter alone
         return launch<SwarPol<B, false, true>>(p, ws, ws_bytes, stream);
-    if (!p.has_out && !p.mask_out)  // a count and at most one aggregate
+    if (!p.has_out && !p.mask_out) {  // a count and at most one aggregate
+        // at 1-4 bits a count or a sum with no input mask takes runs of 8 slabs
+        if constexpr (B <= kSwarPlaneMax)
+            if (!p.has_mask_in && (!p.has_agg || p.agg == AMX_AGG_SUM))
+                return launch<SwarPol<B, false, false, true, false, true>>(p, ws, ws_bytes, stream);
         return launch<SwarPol<B, false, false, true>>(p, ws, ws_bytes, stream);
+    }
     if constexpr (B <= 16) {
         // the plain compressstore takes the kernel that carries only its own path; with an input
         // mask in its 16-warp form: the 24-warp form's two stages and two survivor slots fill the
