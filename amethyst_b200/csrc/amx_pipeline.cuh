@@ -687,15 +687,15 @@ __global__ void __launch_bounds__(Pol::kCompute + kCtlThreads, Pol::kMinBlocks)
             else if constexpr (Pol::kAggOnly) {
                 if (p.has_agg) {
                     bool done = false;
-                    if constexpr (B <= kSwarPlaneMax) {
-                        if (p.agg == AMX_AGG_SUM) {
-                            my_agg += swar_plane_sum<B, SPT>(x, g);
+                    if constexpr (swar_sum_fits<B, SPT>()) {
+                        if (p.agg == AMX_AGG_SUM) {  // field-parallel: no field extracted
+                            my_agg += swar_masked_sum<B, SPT>(x, g);
                             done = true;
                         }
                     }
-                    else if constexpr (swar_sum_fits<B, SPT>()) {
-                        if (p.agg == AMX_AGG_SUM) {  // field-parallel: no field extracted
-                            my_agg += swar_masked_sum<B, SPT>(x, g);
+                    else if constexpr (B <= kSwarPlaneMax) {
+                        if (p.agg == AMX_AGG_SUM) {
+                            my_agg += swar_plane_sum<B, SPT>(x, g);
                             done = true;
                         }
                     }

@@ -278,10 +278,11 @@ __device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], co
 }
 
 // Sum of the passing fields by bit planes, for the narrow widths whose lanes swar_masked_sum cannot
-// hold: the passing fields (whole-field masks as there) are counted per bit position b and each
-// count weighted by 2^b.  B population counts per word, nothing to overflow.  Up to 4 bits (1 GiB-
-// class column, 671M fields, no predicate: 3 bits 0.157 vs 0.479 ms with the compile-time policy);
-// at 7 bits the field visit is faster (0.263 vs 0.312 ms), at 9 the compile-time policy.
+// hold (3 bits): the passing fields (whole-field masks as there) are counted per bit position b and
+// each count weighted by 2^b.  B population counts per word, nothing to overflow.  671M-field
+// column, no predicate, 3 bits: 0.083 ms against 0.481 with the compile-time policy (at 4 bits the
+// lanes beat the planes, 0.100 vs 0.118 ms; at 7 bits the field visit, 0.263 vs 0.312 ms; at 9 the
+// compile-time policy).  kSwarPlaneMax is also the widest width of the wide count-and-sum variant.
 constexpr int kSwarPlaneMax = 4;
 
 template <int B, int SPT>
