@@ -11,6 +11,7 @@ larger than the 126 MB L2 unless the case says otherwise.
   fcB        filter v < 205 * 2^(B-11) + compressstore over 2^24 slabs of width B (e.g. fc11)
   fc_cfg1    filter v < 205 + compressstore over 2^24 elements in 11-bit slabs (26.8 MB)
   filterB    filter -> bitmask over 2^24 slabs of width B
+  sumB       sum of every value of 2^24 slabs of width B (amx_reduce: no predicate, no mask)
   matmul     4096^3 u7 x u7 slab matrices -> narrowest-width slabs (unpack + GEMM + pack)
   matmul_fused  the same through the fused kernel (amx_tuning.policy 2)
   batch64    64 slab columns, lengths log-uniform in [2^16, 2^22], widths 1..32: one batch run
@@ -74,6 +75,20 @@ def case(name: str, reps: int = 10) -> dict:
         ms = _time(step, reps)
         byts = a.nbytes + b.nbytes + ops.storage_bytes(A.SLAB, 14, int(cnt[0].item())) + 16
         return {"case": name, "ms": ms, "GB_s": byts / ms / 1e6}
+    if name.startswith("sum"):
+        bits = int(name[3:])
+        n = (1 << 24) * (64 // bits)
+        col = _gen(n, bits, 0xC0FFEE)
+        ws = ops.workspace(n)
+        res = torch.zeros(2, dtype=torch.int64, device="cuda")
+        cd = col.desc
+
+        def step():
+            A.check(L.amx_reduce(A.AGG_SUM, C.byref(cd), None, C.c_void_p(res.data_ptr()), C.c_void_p(ws.data_ptr()),
+                                 ws.numel(), s))
+
+        ms = _time(step, reps)
+        return {"case": name, "ms": ms, "GB_s": (col.nbytes + 8) / ms / 1e6}
     if name.startswith("fc") or name.startswith("filter"):
         flt = name.startswith("filter")
         small = name == "fc_cfg1"  # the plain configuration: 2^24 elements (not slabs) at 11 bits
