@@ -255,9 +255,10 @@ constexpr int kSwarPolicyBase = 200;
 // A request the field-parallel slab policy (SwarPol) serves: one slab column of width <= 32, a
 // predicate on the field values themselves and/or an input mask, and a compacted output or none;
 // or a sum alone (every field passes) at a width whose field-parallel or bit-plane sum applies, or
-// at 7 bits (field visit).  1 GiB-class column against the compile-time policy: 11 bits 0.234 vs
-// 0.366 ms, 8 bits 0.178 vs 0.336, 32 bits 0.473 vs 0.763, 3 bits 0.157 vs 0.479, 7 bits 0.263 vs
-// 0.397; at 9 and 21 bits, summed field by field, it measured slower (9 bits 0.482 vs 0.375 ms).
+// at 7 bits (field visit).  671M-element column against the compile-time policy: 11 bits 0.234 vs
+// 0.366 ms, 8 bits 0.178 vs 0.336, 32 bits 0.473 vs 0.763, 1 bit 0.035 vs 0.361, 3 bits 0.083 vs
+// 0.481, 7 bits 0.263 vs 0.397.  At 9 and 21 bits the compile-time policy keeps the sum: bit planes
+// measured 0.482 vs 0.375 ms at 9 bits (the b <= 32 test comes first: the rule divides by 64 / b).
 inline bool swar_applicable(const PipeParams& p)
 {
     const int b = (int)p.a.bits;
