@@ -278,9 +278,10 @@ __device__ __forceinline__ uint64_t swar_masked_sum(const uint64_t (&x)[SPT], co
 }
 
 // Sum of the passing fields by bit planes, for the narrow widths whose lanes swar_masked_sum cannot
-// hold (3 bits): the passing fields (whole-field masks as there) are counted per bit position b and
-// each count weighted by 2^b.  B population counts per word, nothing to overflow.  671M-field
-// column, no predicate, 3 bits: 0.083 ms against 0.481 with the compile-time policy (at 4 bits the
+// hold at the policy's SPT (3 bits; 1-3 bits with the wide variant's 8 slabs per thread): the
+// passing fields (whole-field masks as there) are counted per bit position b and each count weighted
+// by 2^b.  B population counts per word, nothing to overflow.  671M-field column, no predicate:
+// 1 bit 0.035 ms, 3 bits 0.083 against 0.361 and 0.481 with the compile-time policy (at 4 bits the
 // lanes beat the planes, 0.100 vs 0.118 ms; at 7 bits the field visit, 0.263 vs 0.312 ms; at 9 the
 // compile-time policy).  kSwarPlaneMax is also the widest width of the wide count-and-sum variant.
 constexpr int kSwarPlaneMax = 4;

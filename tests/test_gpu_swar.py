@@ -181,7 +181,7 @@ def test_swar_mask_input(cuda, restore_tuning, bits):
 
 @pytest.mark.parametrize("bits", list(range(1, 33)))
 def test_sum_alone_every_width(cuda, restore_tuning, bits):
-    """A sum with neither predicate nor mask (field-parallel lanes, bit planes at 3 bits, a field
+    """A sum with neither predicate nor mask (field-parallel lanes, bit planes at 1-3 bits, a field
     visit or the compile-time policy, by width): random columns and columns of maximal fields,
     ragged tails, against the oracle bit-exact; forced and automatic policy choice agree."""
     from amethyst_b200 import _capi as A

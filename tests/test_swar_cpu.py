@@ -128,7 +128,7 @@ def test_field_parallel_masked_sum():
 def test_bit_plane_sum():
     """swar_plane_sum: the passing fields' bits counted per bit position b and weighted by 2^b,
     against field-by-field sums, for the narrow widths up to 9 bits (the kernel takes it where the
-    lanes do not fit: 3 bits)."""
+    lanes do not fit at its run length: 3 bits, or 1-3 bits with runs of 8 slabs)."""
     rng = np.random.default_rng(4)
     for b in range(1, 10):
         e = 64 // b
