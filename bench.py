@@ -595,6 +595,51 @@ def cluster_mask(n, sel, clusters, dev):
     return m.to(torch.int32)
 
 
+def sums_671m(dev, steps):
+    """Sum of every value of a 671,088,640-element slab column (amx_reduce, no predicate, no mask)
+    at several widths: the automatic choice (field-parallel kernels where they apply) against the
+    compile-time-width policy forced through amx_tuning.policy, results compared."""
+    import ctypes as C
+
+    import torch
+
+    from amethyst_b200 import _capi as A
+    from amethyst_b200 import ops
+
+    L = A.lib()
+    stream = torch.cuda.current_stream()
+    s = C.c_void_p(stream.cuda_stream)
+    n = 671088640
+    k = max(3, min(steps, 20))
+    res = torch.zeros(2, dtype=torch.int64, device=dev)
+    rows = {}
+    try:
+        for bits in (1, 3, 4, 7, 8, 11, 16, 32):
+            col = pack_gpu(n, bits, 0x5A + bits, 2)
+            ws = ops.workspace(n)
+            out = {}
+            for name, pol in (("auto", 0), ("compile_time", 1 + bits)):
+                A.check(L.amx_set_tuning(C.byref(A.Tuning(0, 0, pol, 0))) if pol else L.amx_set_tuning(None))
+
+                def step():
+                    A.check(L.amx_reduce(A.AGG_SUM, C.byref(col.desc), None, C.c_void_p(res.data_ptr()),
+                                         C.c_void_p(ws.data_ptr()), ws.numel(), s))
+
+                tot, _ = time_steps(step, k, 3, stream)
+                out[name] = (tot / k, int(res[0].item()))
+            A.check(L.amx_set_tuning(None))
+            ms = out["auto"][0]
+            rows[f"{bits}_bit"] = {"ms": round(ms, 4), "compile_time_ms": round(out["compile_time"][0], 4),
+                                   "GB_s": round(col.nbytes / (ms * 1e-3) / 1e9, 1),
+                                   "identical": out["auto"][1] == out["compile_time"][1]}
+            del col, ws
+            torch.cuda.empty_cache()
+    finally:
+        A.check(L.amx_set_tuning(None))
+    return {"workload": "sum of a 671,088,640-element slab column, automatic kernel vs compile-time-width policy",
+            "rows": rows}
+
+
 def compressstore_masks(dev, steps):
     """compressstore of 2^27 elements in 11-bit slabs by a given mask, for the reference's mask
     distributions (src/main.cu:33-108, run.sh:6-22): uniform random bits, one cluster, eight
@@ -880,6 +925,10 @@ def run_gpu(args):
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["batched_512"] = {"error": str(e)}
             try:
+                extra["sums_671m"] = sums_671m(dev, args.steps)
+            except Exception as e:  # pragma: no cover - reported, not fatal
+                extra["sums_671m"] = {"error": str(e)}
+            try:
                 extra["compressstore_masks"] = compressstore_masks(dev, args.steps)
             except Exception as e:  # pragma: no cover - reported, not fatal
                 extra["compressstore_masks"] = {"error": str(e)}
@@ -970,7 +1019,7 @@ def main():
         dev = torch.device("cuda", 0)
         fn = {"mixed_chain": lambda d, k: mixed_chain(d, k, lanes=args.lanes), "batched_512": batched_512,
               "groupby_2e28": groupby_2e28, "groupby_wide": groupby_wide, "matmul_4096": matmul_4096, "fc_cfg1": fc_cfg1,
-              "compressstore_masks": compressstore_masks,
+              "compressstore_masks": compressstore_masks, "sums_671m": sums_671m,
               "fc_1gib": lambda d, k: fc_1gib(d, max(3, min(k, 30)), 3)}[args.only]
         print(json.dumps({args.only: fn(dev, args.steps)}), flush=True)
     else:
